@@ -1,0 +1,316 @@
+#!/usr/bin/env python
+"""Benchmark of the projector pair at 512^3 (one JSON line on rank 0).
+
+Workload (the metric configuration): float32 512^3 volume @ 0.5 mm (256 mm),
+random-ellipsoid phantom (seed = rank), cone beam DSO 1000 mm / DSD 1536 mm,
+1024 x 768 detector @ 0.4 mm, 720 views over 2 pi.  One step = Siddon forward
+projection of all 720 views + matched backprojection of the 720 projections,
+device-resident (inputs larger than L2, so no flush is needed).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value      GRays/s of the Siddon projection (rays of all ranks / max device time)
+atb        Gvox-upd/s of the matched backprojection
+e2e        the same metrics through the public host API (numpy in, numpy out:
+           host->device and device->host copies inside the timed region)
+roofline   dominant kernel, algorithmic bytes / CUDA-event duration vs measured HBM
+cpu_baseline  the FP64 oracle on a bounded sample of views, all host cores
+--impl reference  the reference's own CUDA build (oracle/_ref) through its own
+           host-pointer C++ entry points, in a child process
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NV, NU, NA = 768, 1024, 720
+NVOX = (512, 512, 512)
+METRIC = "GRays/s Ax + Gvox-upd/s Atb at 512^3"
+WORKLOAD = "cone-beam 512^3 @ 0.5 mm, 1024x768 det @ 0.4 mm, 720 views / 2pi, DSO 1000, DSD 1536"
+
+
+def geometry():
+    from tigre_b200.utilities.geometry import cone_geometry
+    return cone_geometry(NVOX, (256.0, 256.0, 256.0), (NV, NU), (0.4, 0.4), DSO=1000.0, DSD=1536.0)
+
+
+def angles():
+    return np.linspace(0, 2 * np.pi, NA, endpoint=False).astype(np.float32)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling (200 ms) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(geo, ang, n_views=4):
+    """FP64 oracle on n_views evenly spaced views, full detector, all host cores."""
+    from oracle import oracle as O
+    idx = np.linspace(0, NA, n_views, endpoint=False).astype(int)
+    sub = ang[idx]
+    img = _phantom_host(0)
+    t = time.perf_counter()
+    O.ax(img, geo, sub, "Siddon")
+    dt = time.perf_counter() - t
+    rays = n_views * NU * NV
+    return {"value": rays / dt / 1e9, "unit": "GRays/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": "FP64 oracle Siddon, %d of %d views, full %dx%d detector, %.1f s" % (n_views, NA, NU, NV, dt)}
+
+
+_PH = {}
+
+
+def _phantom_host(seed):
+    if seed not in _PH:
+        import torch
+        from tigre_b200.utilities.phantom import random_ellipsoids
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+        _PH[seed] = random_ellipsoids(NVOX, seed=seed, device=dev).cpu().numpy()
+    return _PH[seed]
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from oracle import ref
+    geo, ang = geometry(), angles()
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference CUDA build (oracle/_ref) not present"}))
+        return
+    img = _phantom_host(0)
+    reps = args.warmup + args.steps
+    proj, t_ax = ref.ax(img, geo, ang, "Siddon", repeat=reps)
+    _, t_atb = ref.atb(proj, geo, ang, "matched", repeat=reps)
+    t_ax, t_atb = t_ax[args.warmup:], t_atb[args.warmup:]
+    rays, upd = NA * NU * NV, NA * math.prod(NVOX)
+    v = rays / statistics.median(t_ax) / 1e9
+    va = upd / statistics.median(t_atb) / 1e9
+    b_in, b_out = math.prod(NVOX) * 4, NA * NU * NV * 4
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": "GRays/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * (statistics.median(t_ax) + statistics.median(t_atb)), 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "reference": "TIGRE Common/CUDA built for sm_100a, host-pointer API "
+                                                      "siddon_ray_projection + voxel_backprojection2"},
+        "atb": {"value": round(va, 4), "unit": "Gvox-upd/s"},
+        "e2e": {"value": round(v, 4), "unit": "GRays/s", "atb_value": round(va, 4), "atb_unit": "Gvox-upd/s",
+                "h2d_bytes_per_step": b_in + b_out, "d2h_bytes_per_step": b_out + b_in},
+        "cpu_baseline": {"kind": "reference", "cores": os.cpu_count(), "value": round(v, 4), "unit": "GRays/s",
+                         "sample": "full workload; the reference has no CPU projector, its CUDA build runs on the GPU"},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from tigre_b200 import _native as N, projectors as P
+
+    dev = torch.device("cuda", local)
+    geo, ang = geometry(), angles()
+    plan = N.get_plan(N.checked_geometry(geo, ang), local)
+    from tigre_b200.utilities.phantom import random_ellipsoids
+    vol = random_ellipsoids(NVOX, seed=rank, device=dev)
+    proj = torch.empty((NA, NV, NU), dtype=torch.float32, device=dev)
+    bp = torch.empty_like(vol)
+    nseg = P.siddon_segments(plan)
+    for _ in range(max(3, args.warmup)):
+        P.ax(vol, plan, "Siddon", out=proj)
+        P.atb(proj, plan, "matched", out=bp)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = Clocks(local)
+    clk.start()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        ev[k][0].record()
+        P.ax(vol, plan, "Siddon", out=proj)
+        ev[k][1].record()
+        P.atb(proj, plan, "matched", out=bp)
+        ev[k][2].record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = clk.stop()
+    t_ax = sum(e[0].elapsed_time(e[1]) for e in ev) / 1e3
+    t_atb = sum(e[1].elapsed_time(e[2]) for e in ev) / 1e3
+    t_tot = ev[0][0].elapsed_time(ev[-1][2]) / 1e3
+    if dist:
+        t = torch.tensor([t_ax, t_atb, t_tot], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ax, t_atb, t_tot = t.tolist()
+    rays = NA * NU * NV
+    upd = NA * math.prod(NVOX)
+    value = world * rays * args.steps / t_ax / 1e9
+    atb_value = world * upd * args.steps / t_atb / 1e9
+    # roofline of the dominant kernel, algorithmic bytes per launch
+    peak, peak_kind = peaks()
+    ax_launch = t_ax / args.steps
+    atb_launch = t_atb / args.steps
+    if ax_launch >= atb_launch:
+        alg = nseg * 4 + rays * 4           # one voxel gather per Siddon segment + one output write per ray
+        roof = {"kernel": "siddon_kernel<float,float>", "bound": "hbm", "achieved": alg / ax_launch / 1e9,
+                "alg_bytes_per_launch": alg}
+    else:
+        alg = upd * 4 * 4 + math.prod(NVOX) * 4   # 4 bilinear taps per update + one volume write
+        roof = {"kernel": "bp_kernel<matched>", "bound": "hbm", "achieved": alg / atb_launch / 1e9,
+                "alg_bytes_per_launch": alg}
+    roof.update({"peak": peak, "unit": "GB/s", "frac": roof["achieved"] / peak, "peak_source": peak_kind,
+                 "traffic": None})
+    for k in ("achieved", "frac"):
+        roof[k] = round(roof[k], 4)
+    e2e = None
+    if not args.no_e2e and rank == 0:
+        e2e = measure_e2e(vol, geo, ang, min(args.steps, 3))
+    if dist:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": "GRays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": round(1e3 * t_tot / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded random ellipsoids)",
+            "config": {"workload": WORKLOAD, "step": "Siddon Ax of 720 views + matched Atb",
+                       "l2": "inputs larger than L2 (volume 512 MiB, projections 2.1 GiB)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "atb": {"value": round(atb_value, 4), "unit": "Gvox-upd/s", "ms_per_launch": round(1e3 * atb_launch, 3)},
+            "ax_ms_per_launch": round(1e3 * ax_launch, 3),
+            "siddon_segments": nseg,
+            "roofline": roof,
+            "gpu_launches": 4 * args.steps,
+            "clocks": clocks,
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if not args.no_cpu:
+            try:
+                line["cpu_baseline"] = cpu_baseline(geo, ang)
+            except Exception as ex:  # the baseline must not hide the GPU result
+                line["cpu_baseline"] = {"error": str(ex)[:200]}
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def measure_e2e(vol, geo, ang, steps):
+    """Public host API: pinned numpy in, numpy out, copies inside the timed region."""
+    import torch
+    import tigre_b200 as tigre
+    img = torch.empty(vol.shape, dtype=torch.float32, pin_memory=True)
+    img.copy_(vol)
+    img_np = img.numpy()
+    tigre.Ax(img_np, geo, ang, "Siddon")    # warm-up (plan, pools)
+    ta, tb = [], []
+    proj_np = None
+    for _ in range(steps):
+        t = time.perf_counter()
+        proj_np = tigre.Ax(img_np, geo, ang, "Siddon")
+        ta.append(time.perf_counter() - t)
+    pin = torch.empty(proj_np.shape, dtype=torch.float32, pin_memory=True)
+    pin.copy_(torch.from_numpy(proj_np))
+    pin_np = pin.numpy()
+    tigre.Atb(pin_np, geo, ang, "matched")
+    for _ in range(steps):
+        t = time.perf_counter()
+        tigre.Atb(pin_np, geo, ang, "matched")
+        tb.append(time.perf_counter() - t)
+    rays, upd = NA * NU * NV, NA * math.prod(NVOX)
+    b_vol, b_proj = math.prod(NVOX) * 4, NA * NU * NV * 4
+    return {"value": round(rays / statistics.median(ta) / 1e9, 4), "unit": "GRays/s",
+            "atb_value": round(upd / statistics.median(tb) / 1e9, 4), "atb_unit": "Gvox-upd/s",
+            "ax_s": round(statistics.median(ta), 4), "atb_s": round(statistics.median(tb), 4),
+            "h2d_bytes_per_step": b_vol + b_proj, "d2h_bytes_per_step": b_proj + b_vol}
+
+
+if __name__ == "__main__":
+    main()

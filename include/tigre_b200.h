@@ -1,0 +1,183 @@
+/*
+ * tigre_b200.h -- C ABI of libtigre_b200.so, the sm_100a projector pair.
+ *
+ * Two layers of entry points live in the same shared library:
+ *
+ *  1. Drop-in host-pointer calls with the reference's argument meaning and
+ *     error codes.  Each replaces one reference function of TIGRE's
+ *     Common/CUDA layer (cited per declaration).  They take host pointers,
+ *     block until the result is in host memory, and return 0 on success or a
+ *     code of Common/CUDA/errors.hpp:1-7 (they never exit the process, unlike
+ *     the reference's mexErrMsgIdAndTxt, TIGRE_common.cpp:13-16).
+ *     C++ callers that bind the reference's exact C++ signatures (the unmodified
+ *     Cython _Ax/_Atb/_minTV extensions) use include/tigre_b200_compat.hpp,
+ *     whose functions are exported by the same library.
+ *
+ *  2. A device-resident API (plan + device pointers + CUDA stream) used by the
+ *     Python package for algorithms, autograd and benchmarks.  It has no
+ *     counterpart in the reference, whose every call copies host<->device.
+ *
+ * All pointers are plain pointers; streams are passed as void* (cudaStream_t).
+ */
+#ifndef TIGRE_B200_H
+#define TIGRE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes, values of Common/CUDA/errors.hpp:1-7. */
+#define TIGRE_SUCCESS 0
+#define TIGRE_ERR_CUDA 1
+#define TIGRE_ERR_NO_CAPABLE_DEVICES 2
+#define TIGRE_ERR_NO_FREE_DEVICES 3
+#define TIGRE_ERR_BAD_ASSERT 4
+#define TIGRE_ERR_ASSERT_FAIL 5
+
+/* Storage types accepted by the device API (arithmetic is always FP32, geometry FP64). */
+#define TIGRE_F32 0
+#define TIGRE_BF16 1
+#define TIGRE_F16 2
+
+/* Projector / backprojector selectors. */
+#define TIGRE_PROJ_SIDDON 0
+#define TIGRE_PROJ_INTERPOLATED 1
+#define TIGRE_BACKPROJ_FDK 0
+#define TIGRE_BACKPROJ_MATCHED 1
+
+/*
+ * Per-call geometry: field-for-field the layout of `struct Geometry`
+ * (Common/CUDA/types_TIGRE.hpp:48-85).  Per-angle arrays have nangles entries.
+ * Axes are in the C convention: X fastest, detector U fastest.
+ */
+typedef struct TigreGeometry {
+    int nVoxelX, nVoxelY, nVoxelZ;
+    float sVoxelX, sVoxelY, sVoxelZ;
+    float dVoxelX, dVoxelY, dVoxelZ;
+    float *offOrigX, *offOrigY, *offOrigZ;
+    float *DSO;
+    int nDetecU, nDetecV;
+    float sDetecU, sDetecV;
+    float dDetecU, dDetecV;
+    float *offDetecU, *offDetecV;
+    float *DSD;
+    float *dRoll;
+    float *dPitch;
+    float *dYaw;
+    float unitX, unitY, unitZ;
+    float alpha, theta, psi;
+    float *COR;
+    float maxLength;
+    float accuracy;
+} TigreGeometry;
+
+/* Text of the last error raised on the calling thread ("" if none). */
+const char* tigre_last_error(void);
+/* Library version (major*100 + minor). */
+int tigre_version(void);
+
+/* ---------------------------------------------------------------------------
+ * 1. Drop-in host-pointer entry points.
+ *    gpu_ids/n_gpus: device list of the reference's GpuIds (Common/CUDA/GpuIds.hpp);
+ *    this build runs on gpu_ids[0] (n_gpus == 0 means device 0).
+ * ------------------------------------------------------------------------- */
+
+/* Siddon ray-driven cone-beam projection.  Replaces siddon_ray_projection
+ * (Common/CUDA/Siddon_projection.hpp:97, Siddon_projection.cu:271).
+ * img: (nVoxelZ, nVoxelY, nVoxelX) float32; result[i]: projection i, (nDetecV, nDetecU);
+ * angles: (nangles, 3) ZYZ Euler angles. */
+int tigre_siddon_ray_projection(const float* img, const TigreGeometry* geo, float* const* result,
+                                const float* angles, int nangles, const int* gpu_ids, int n_gpus);
+
+/* Interpolated (fixed-step trilinear) cone-beam projection.  Replaces
+ * interpolation_projection (Common/CUDA/ray_interpolated_projection.hpp:55,
+ * ray_interpolated_projection.cu:211). */
+int tigre_interpolation_projection(const float* img, const TigreGeometry* geo, float* const* result,
+                                   const float* angles, int nangles, const int* gpu_ids, int n_gpus);
+
+/* FDK-weighted voxel backprojection.  Replaces voxel_backprojection
+ * (Common/CUDA/voxel_backprojection.hpp:52, voxel_backprojection.cu:293).
+ * projections: (nangles, nDetecV, nDetecU); result: (nVoxelZ, nVoxelY, nVoxelX), overwritten. */
+int tigre_voxel_backprojection(const float* projections, const TigreGeometry* geo, float* result,
+                               const float* angles, int nangles, const int* gpu_ids, int n_gpus);
+
+/* Matched voxel backprojection (weight L^3/(DSD*|S-x|^2), scaled by dV/dDetArea).
+ * Replaces voxel_backprojection2 (Common/CUDA/voxel_backprojection2.hpp:57,
+ * voxel_backprojection2.cu:318). */
+int tigre_voxel_backprojection2(const float* projections, const TigreGeometry* geo, float* result,
+                                const float* angles, int nangles, const int* gpu_ids, int n_gpus);
+
+/* POCS total-variation descent: maxIter steps of img -= alpha*g/|g|, g = grad TV(img).
+ * Replaces pocs_tv (Common/CUDA/GD_TV.hpp:58, GD_TV.cu:255).  image_size = {nX, nY, nZ}.
+ * Unlike the reference it does not reset the device at the end. */
+int tigre_pocs_tv(const float* img, float* dst, float alpha, const long* image_size, int max_iter,
+                  const int* gpu_ids, int n_gpus);
+
+/* Parallel-beam entry points referenced by the reference's Cython layer
+ * (_Ax.pyx:21-26, _Atb.pyx:21-22: siddon_ray_projection_parallel,
+ * interpolation_projection_parallel, voxel_backprojection_parallel).  Parallel
+ * beam is outside this library: they return TIGRE_ERR_BAD_ASSERT. */
+int tigre_siddon_ray_projection_parallel(const float* img, const TigreGeometry* geo, float* const* result,
+                                         const float* angles, int nangles, const int* gpu_ids, int n_gpus);
+int tigre_interpolation_projection_parallel(const float* img, const TigreGeometry* geo, float* const* result,
+                                            const float* angles, int nangles, const int* gpu_ids, int n_gpus);
+int tigre_voxel_backprojection_parallel(const float* projections, const TigreGeometry* geo, float* result,
+                                        const float* angles, int nangles, const int* gpu_ids, int n_gpus);
+
+/* ---------------------------------------------------------------------------
+ * 2. Device-resident API (no counterpart in the reference).
+ * ------------------------------------------------------------------------- */
+
+/* A plan holds the FP64 per-angle geometry (uploaded once) and reusable device
+ * scratch for the working layouts of one geometry.  Plans are not thread-safe:
+ * use one plan per host thread / stream. */
+typedef struct TigrePlan TigrePlan;
+
+int tigre_plan_create(const TigreGeometry* geo, const float* angles, int nangles, int device, TigrePlan** plan);
+void tigre_plan_destroy(TigrePlan* plan);
+/* Bytes of device scratch currently held by the plan. */
+long long tigre_plan_scratch_bytes(const TigrePlan* plan);
+
+/* Forward projection of d_vol (nZ,nY,nX) into d_proj ((angle_end-angle_begin), nV, nU)
+ * for plan angles [angle_begin, angle_end).  projector: TIGRE_PROJ_*. */
+int tigre_ax(TigrePlan* plan, const void* d_vol, int vol_dtype, void* d_proj, int proj_dtype, int projector,
+             int angle_begin, int angle_end, void* stream);
+
+/* Backprojection of d_proj ((angle_end-angle_begin), nV, nU) into d_vol (overwritten).
+ * backprojector: TIGRE_BACKPROJ_*. */
+int tigre_atb(TigrePlan* plan, const void* d_proj, int proj_dtype, void* d_vol, int vol_dtype, int backprojector,
+              int angle_begin, int angle_end, void* stream);
+
+/* Sum over all rays of the number of Siddon voxel segments (FP64 ray setup only,
+ * no traversal); the algorithmic-bytes count of the Siddon roofline. */
+int tigre_siddon_count_segments(TigrePlan* plan, int angle_begin, int angle_end, unsigned long long* d_total,
+                                void* stream);
+
+/* POCS-TV on a device volume, in place: max_iter steps of GD_TV.cu:440-597.
+ * d_work: caller scratch of nx*ny*nz floats (same dtype as d_img is not required: FP32). */
+int tigre_tv_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha, int max_iter, float* d_work,
+                  void* stream);
+/* TV gradient (GD_TV.cu:117-143, single-device boundary rule) into d_grad (FP32). */
+int tigre_tv_gradient(const void* d_img, int dtype, float* d_grad, long nx, long ny, long nz, void* stream);
+/* TV value sum_i |grad f_i| consistent with tigre_tv_gradient; added into *d_out (FP64). */
+int tigre_tv_value(const void* d_img, int dtype, long nx, long ny, long nz, double* d_out, void* stream);
+
+/* FP64 reductions and fused CGLS updates (device scalars, no host round trip). */
+int tigre_sumsq(const void* d_x, int dtype, long n, double* d_out, void* stream);          /* *d_out += sum x^2 */
+int tigre_dot(const float* d_x, const float* d_y, long n, double* d_out, void* stream);    /* *d_out += sum x*y */
+/* x += a*p; r -= a*q; *d_rr += |r|^2, with a = (*d_num)/(*d_den). */
+int tigre_cgls_step(float* d_x, const float* d_p, long nvol, float* d_r, const float* d_q, long nproj,
+                    const double* d_num, const double* d_den, double* d_rr, void* stream);
+/* p = s + (*d_num / *d_den) * p */
+int tigre_cgls_direction(float* d_p, const float* d_s, long n, const double* d_num, const double* d_den,
+                         void* stream);
+
+/* Type conversion between storage types (for the reduced-precision paths). */
+int tigre_convert(const void* d_src, int src_dtype, void* d_dst, int dst_dtype, long n, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TIGRE_B200_H */

@@ -1,0 +1,69 @@
+// tigre_b200_compat.hpp -- the reference's own C++ entry points, exported by
+// libtigre_b200.so with the exact signatures (and therefore the same mangled
+// symbols) that TIGRE's Cython extensions bind:
+//
+//   Common/CUDA/Siddon_projection.hpp:97          siddon_ray_projection
+//   Common/CUDA/ray_interpolated_projection.hpp:55 interpolation_projection
+//   Common/CUDA/voxel_backprojection.hpp:52       voxel_backprojection
+//   Common/CUDA/voxel_backprojection2.hpp:57      voxel_backprojection2
+//   Common/CUDA/GD_TV.hpp:58                      pocs_tv
+//   and the *_parallel symbols referenced by _Ax.pyx:21-26 / _Atb.pyx:21-22.
+//
+// `Geometry` and `GpuIds` here are declared with the field layout of
+// Common/CUDA/types_TIGRE.hpp:48-85 and Common/CUDA/GpuIds.hpp:2-14 (the
+// library only reads GpuIds' two data members and defines none of its
+// methods, so the extension's own GpuIds.cpp keeps providing them).
+// Include either this header or the reference's headers, never both.
+#ifndef TIGRE_B200_COMPAT_HPP
+#define TIGRE_B200_COMPAT_HPP
+
+#ifndef TYPES_CBCT
+#define TYPES_CBCT
+struct Geometry {
+    int nVoxelX, nVoxelY, nVoxelZ;
+    float sVoxelX, sVoxelY, sVoxelZ;
+    float dVoxelX, dVoxelY, dVoxelZ;
+    float *offOrigX, *offOrigY, *offOrigZ;
+    float* DSO;
+    int nDetecU, nDetecV;
+    float sDetecU, sDetecV;
+    float dDetecU, dDetecV;
+    float *offDetecU, *offDetecV;
+    float* DSD;
+    float* dRoll;
+    float* dPitch;
+    float* dYaw;
+    float unitX, unitY, unitZ;
+    float alpha, theta, psi;
+    float* COR;
+    float maxLength;
+    float accuracy;
+};
+#endif
+
+#ifndef GPUIDS_H
+#define GPUIDS_H
+struct GpuIds {
+    int* m_piDeviceIds;
+    int m_iCount;
+};
+#endif
+
+int siddon_ray_projection(float* img, Geometry geo, float** result, float const* const angles, int nangles,
+                          const GpuIds& gpuids);
+int siddon_ray_projection_parallel(float* img, Geometry geo, float** result, float const* const angles, int nangles,
+                                   const GpuIds& gpuids);
+int interpolation_projection(float* img, Geometry geo, float** result, float const* const angles, int nangles,
+                             const GpuIds& gpuids);
+int interpolation_projection_parallel(float* img, Geometry geo, float** result, float const* const angles,
+                                      int nangles, const GpuIds& gpuids);
+int voxel_backprojection(float* projections, Geometry geo, float* result, float const* const alphas, int nalpha,
+                         const GpuIds& gpuids);
+int voxel_backprojection2(float* projections, Geometry geo, float* result, float const* const alphas, int nalpha,
+                          const GpuIds& gpuids);
+int voxel_backprojection_parallel(float* projections, Geometry geo, float* result, float const* const alphas,
+                                  int nalpha, const GpuIds& gpuids);
+// The reference returns void here; errors are reported on stderr and leave dst unchanged.
+void pocs_tv(float* img, float* dst, float alpha, const long* image_size, int maxIter, const GpuIds& gpuids);
+
+#endif  // TIGRE_B200_COMPAT_HPP

@@ -1,0 +1,159 @@
+"""ctypes front end of the FP64 host oracle (oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, never by the product package.
+
+Geometry conversion follows Python/tigre/utilities/cuda_interface/_types.pxd:69-166
+(axis swap (z,y,x) -> x/y/z, (v,u) -> u/v; rotDetector[:,2]/[1]/[0] -> roll/pitch/yaw)
+after the reference's check_geo() + cast_to_single().
+"""
+from __future__ import annotations
+
+import copy
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_D = C.POINTER(C.c_double)
+
+
+class OGeo(C.Structure):
+    _fields_ = [
+        ("nVoxelX", C.c_int), ("nVoxelY", C.c_int), ("nVoxelZ", C.c_int),
+        ("sVoxelX", C.c_double), ("sVoxelY", C.c_double), ("sVoxelZ", C.c_double),
+        ("dVoxelX", C.c_double), ("dVoxelY", C.c_double), ("dVoxelZ", C.c_double),
+        ("nDetecU", C.c_int), ("nDetecV", C.c_int),
+        ("sDetecU", C.c_double), ("sDetecV", C.c_double),
+        ("dDetecU", C.c_double), ("dDetecV", C.c_double),
+        ("accuracy", C.c_double),
+        ("nangles", C.c_int),
+        ("offOrigX", _D), ("offOrigY", _D), ("offOrigZ", _D),
+        ("offDetecU", _D), ("offDetecV", _D),
+        ("DSO", _D), ("DSD", _D),
+        ("dRoll", _D), ("dPitch", _D), ("dYaw", _D),
+        ("COR", _D),
+        ("alpha", _D), ("theta", _D), ("psi", _D),
+    ]
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "_build", "liboracle.so")
+        if not os.path.exists(path):
+            import importlib.util
+            spec = importlib.util.spec_from_file_location("_oracle_build", os.path.join(_HERE, "build.py"))
+            mod = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(mod)
+            mod.build_oracle()
+        _LIB = C.CDLL(path)
+        f = C.c_void_p
+        _LIB.oracle_siddon.argtypes = [f, C.POINTER(OGeo), C.c_int, C.c_int, C.c_int, C.c_int, f, f, C.c_int]
+        _LIB.oracle_interp.argtypes = [f, C.POINTER(OGeo), C.c_int, C.c_int, C.c_int, C.c_int, f, f, C.c_int]
+        _LIB.oracle_backproject.argtypes = [f, C.POINTER(OGeo), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, f,
+                                            C.c_int]
+        _LIB.oracle_tv_gradient.argtypes = [f, C.c_long, C.c_long, C.c_long, f, C.c_int]
+        _LIB.oracle_pocs_tv.argtypes = [f, f, C.c_float, C.c_long, C.c_long, C.c_long, C.c_int, C.c_int]
+    return _LIB
+
+
+class _Geo:
+    """Keeps the per-angle double arrays alive while the C struct points at them."""
+
+    def __init__(self, geo, angles):
+        g = copy.deepcopy(geo)
+        g.check_geo(angles)
+        g.cast_to_single()
+        n = g.angles.shape[0]
+        self.n = n
+        keep = {}
+
+        def arr(v):
+            a = np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(n))
+            keep[id(a)] = a
+            return a.ctypes.data_as(_D)
+
+        off = np.asarray(g.offOrigin, dtype=np.float64).reshape(n, 3)
+        offd = np.asarray(g.offDetector, dtype=np.float64).reshape(n, 2)
+        rot = np.asarray(g.rotDetector, dtype=np.float64).reshape(n, 3)
+        ang = np.asarray(g.angles, dtype=np.float32).astype(np.float64).reshape(n, 3)
+        s = OGeo()
+        s.nVoxelX, s.nVoxelY, s.nVoxelZ = int(g.nVoxel[2]), int(g.nVoxel[1]), int(g.nVoxel[0])
+        s.sVoxelX, s.sVoxelY, s.sVoxelZ = float(g.sVoxel[2]), float(g.sVoxel[1]), float(g.sVoxel[0])
+        s.dVoxelX, s.dVoxelY, s.dVoxelZ = float(g.dVoxel[2]), float(g.dVoxel[1]), float(g.dVoxel[0])
+        s.nDetecU, s.nDetecV = int(g.nDetector[1]), int(g.nDetector[0])
+        s.sDetecU, s.sDetecV = float(g.sDetector[1]), float(g.sDetector[0])
+        s.dDetecU, s.dDetecV = float(g.dDetector[1]), float(g.dDetector[0])
+        s.accuracy = float(g.accuracy)
+        s.nangles = n
+        s.offOrigX, s.offOrigY, s.offOrigZ = arr(off[:, 2]), arr(off[:, 1]), arr(off[:, 0])
+        s.offDetecU, s.offDetecV = arr(offd[:, 1]), arr(offd[:, 0])
+        s.DSO, s.DSD = arr(g.DSO), arr(g.DSD)
+        s.dRoll, s.dPitch, s.dYaw = arr(rot[:, 2]), arr(rot[:, 1]), arr(rot[:, 0])
+        s.COR = arr(g.COR)
+        s.alpha, s.theta, s.psi = arr(ang[:, 0]), arr(ang[:, 1]), arr(ang[:, 2])
+        self.s = s
+        self._keep = keep
+        self.g = g
+
+
+def _threads(nthreads):
+    return int(nthreads) if nthreads else (os.cpu_count() or 1)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def ax(img, geo, angles, projection_type="Siddon", angle_range=None, row_range=None, nthreads=0,
+       return_counts=False):
+    """FP64 forward projection.  Returns (nA, nR, nU) float32 for the selected angles/rows
+    (and the per-ray segment/sample counts when return_counts)."""
+    G = _Geo(geo, angles)
+    s = G.s
+    a0, a1 = angle_range if angle_range is not None else (0, G.n)
+    v0, v1 = row_range if row_range is not None else (0, s.nDetecV)
+    img = _f32(img)
+    assert img.shape == (s.nVoxelZ, s.nVoxelY, s.nVoxelX)
+    out = np.zeros((a1 - a0, v1 - v0, s.nDetecU), dtype=np.float32)
+    cnt = np.zeros(out.shape, dtype=np.int32) if return_counts else None
+    fn = lib().oracle_siddon if projection_type in ("Siddon", "ray-voxel") else lib().oracle_interp
+    fn(img.ctypes.data, C.byref(s), a0, a1, v0, v1, out.ctypes.data,
+       cnt.ctypes.data if cnt is not None else None, _threads(nthreads))
+    return (out, cnt) if return_counts else out
+
+
+def atb(proj, geo, angles, backprojection_type="FDK", angle_range=None, z_range=None, nthreads=0):
+    """FP64 voxel backprojection of proj (nA, nV, nU).  Returns (nz, nY, nX) float32."""
+    G = _Geo(geo, angles)
+    s = G.s
+    a0, a1 = angle_range if angle_range is not None else (0, G.n)
+    z0, z1 = z_range if z_range is not None else (0, s.nVoxelZ)
+    proj = _f32(proj)
+    assert proj.shape == (G.n, s.nDetecV, s.nDetecU)
+    out = np.zeros((z1 - z0, s.nVoxelY, s.nVoxelX), dtype=np.float32)
+    matched = 1 if backprojection_type == "matched" else 0
+    lib().oracle_backproject(proj.ctypes.data, C.byref(s), a0, a1, z0, z1, matched, out.ctypes.data,
+                             _threads(nthreads))
+    return out
+
+
+def tv_gradient(img, nthreads=0):
+    img = _f32(img)
+    nz, ny, nx = img.shape
+    out = np.empty_like(img)
+    lib().oracle_tv_gradient(img.ctypes.data, nx, ny, nz, out.ctypes.data, _threads(nthreads))
+    return out
+
+
+def pocs_tv(img, alpha, maxiter, nthreads=0):
+    img = _f32(img)
+    nz, ny, nx = img.shape
+    out = np.empty_like(img)
+    lib().oracle_pocs_tv(img.ctypes.data, out.ctypes.data, float(alpha), nx, ny, nz, int(maxiter),
+                         _threads(nthreads))
+    return out

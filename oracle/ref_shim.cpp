@@ -1,0 +1,68 @@
+// extern "C" shim over the reference's own C++ entry points.
+//
+// TEST INFRASTRUCTURE ONLY.  oracle/build_ref.py compiles this file together
+// with the reference's CUDA sources (read in place from the TIGRE tree, never
+// copied) into oracle/_ref/libref_{ax,atb,tv}.so, grouped exactly as the
+// reference's own Python extensions group them (setup.py:347-433).  The
+// wrappers take a single device id and build the GpuIds object the reference
+// expects (Common/CUDA/GpuIds.hpp).  The reference calls exit(1) on any CUDA
+// error (Common/CUDA/TIGRE_common.cpp:13-16), so callers must load these
+// libraries in a child process (oracle/ref.py does).
+
+#include <cstdlib>
+#include "types_TIGRE.hpp"
+#include "GpuIds.hpp"
+
+#if defined(REF_AX)
+#include "Siddon_projection.hpp"
+#include "ray_interpolated_projection.hpp"
+#elif defined(REF_ATB)
+#include "voxel_backprojection.hpp"
+#include "voxel_backprojection2.hpp"
+#elif defined(REF_TV)
+#include "GD_TV.hpp"
+#endif
+
+namespace {
+struct OneGpu {
+    GpuIds ids;
+    explicit OneGpu(int dev) { ids.SetIds(1, &dev); }
+};
+}  // namespace
+
+extern "C" {
+
+#if defined(REF_AX)
+// projector: 0 = Siddon (siddon_ray_projection, Siddon_projection.cu:271),
+//            1 = interpolated (interpolation_projection, ray_interpolated_projection.cu:211)
+int ref_ax(float* img, const Geometry* geo, float* out, const float* angles, int nangles, int projector, int dev) {
+    OneGpu g(dev);
+    const size_t npix = (size_t)geo->nDetecU * (size_t)geo->nDetecV;
+    float** rows = (float**)std::malloc(sizeof(float*) * (size_t)nangles);
+    if (!rows) return 1;
+    for (int i = 0; i < nangles; ++i) rows[i] = out + npix * (size_t)i;
+    int rc = projector == 0 ? siddon_ray_projection(img, *geo, rows, angles, nangles, g.ids)
+                            : interpolation_projection(img, *geo, rows, angles, nangles, g.ids);
+    std::free(rows);
+    return rc;
+}
+#elif defined(REF_ATB)
+// backprojector: 0 = FDK (voxel_backprojection, voxel_backprojection.cu:293),
+//                1 = matched (voxel_backprojection2, voxel_backprojection2.cu:318)
+int ref_atb(float* proj, const Geometry* geo, float* out, const float* angles, int nangles, int backprojector,
+            int dev) {
+    OneGpu g(dev);
+    return backprojector == 0 ? voxel_backprojection(proj, *geo, out, angles, nangles, g.ids)
+                              : voxel_backprojection2(proj, *geo, out, angles, nangles, g.ids);
+}
+#elif defined(REF_TV)
+// pocs_tv (GD_TV.cu:255); image_size = {nX, nY, nZ}.  Note that the reference
+// ends this call with cudaDeviceReset().
+int ref_pocs_tv(float* img, float* dst, float alpha, const long* image_size, int maxiter, int dev) {
+    OneGpu g(dev);
+    pocs_tv(img, dst, alpha, image_size, maxiter, g.ids);
+    return 0;
+}
+#endif
+
+}  // extern "C"

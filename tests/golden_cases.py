@@ -1,0 +1,26 @@
+"""Small seeded cases whose reference outputs are stored in tests/golden/."""
+import numpy as np
+
+from tigre_b200.utilities.geometry import cone_geometry
+from tigre_b200.utilities.phantom import random_ellipsoids
+
+TV_ALPHA = 0.002
+TV_ITERS = 10
+
+CASES = ("small", "offsets")
+
+
+def make(name):
+    if name == "small":
+        geo = cone_geometry((32, 32, 32), (32.0, 32.0, 32.0), (48, 64), (0.8, 0.8))
+        ang = np.linspace(0, 2 * np.pi, 12, endpoint=False).astype(np.float32)
+        img = random_ellipsoids((32, 32, 32), seed=21)
+    elif name == "offsets":
+        geo = cone_geometry((24, 30, 28), (24 * 1.1, 30 * 0.9, 28.0), (40, 52), (0.9, 0.7))
+        geo.offOrigin = np.array((1.0, -1.5, 2.0))
+        geo.offDetector = np.array((1.2, -0.8))
+        ang = np.linspace(0.1, 1.7 * np.pi, 10, endpoint=False).astype(np.float32)
+        img = random_ellipsoids((24, 30, 28), seed=22)
+    else:
+        raise KeyError(name)
+    return geo, ang, img.astype(np.float32)

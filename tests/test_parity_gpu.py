@@ -1,0 +1,180 @@
+"""Parity of the sm_100a projector pair with the FP64 oracle, through the C ABI.
+
+Bar (FP32 storage, FP64 geometry, exact interpolation): max|gpu-oracle| / max|oracle|
+and ||gpu-oracle|| / ||oracle|| both <= TOL = 1e-5.
+"""
+import numpy as np
+import pytest
+
+from tests import geometries as G
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _torch():
+    import torch
+    return torch
+
+
+CASES = {
+    "c1": (G.c1_geometry, lambda: G.angles(100), 0),
+    "odd": (G.odd_geometry, lambda: G.angles(37, full=np.pi * 1.3), 1),
+    "tilted": (G.tilted_geometry, lambda: G.angles(23, tilt=True), 2),
+}
+
+
+@pytest.fixture(scope="module", params=list(CASES))
+def case(request):
+    mk_geo, mk_ang, seed = CASES[request.param]
+    geo = mk_geo()
+    ang = mk_ang()
+    img = G.phantom(tuple(int(v) for v in geo.nVoxel), seed=seed)
+    return request.param, geo, ang, img
+
+
+@pytest.mark.parametrize("ptype", ["Siddon", "interpolated"])
+def test_ax_host_api_matches_oracle(case, ptype):
+    import tigre_b200 as tigre
+    name, geo, ang, img = case
+    got = tigre.Ax(img, geo, ang, ptype)
+    ref = O.ax(img, geo, ang, ptype)
+    mx, l2 = G.rel_err(got, ref)
+    assert mx <= TOL and l2 <= TOL, (name, ptype, mx, l2)
+
+
+@pytest.mark.parametrize("btype", ["FDK", "matched"])
+def test_atb_host_api_matches_oracle(case, btype):
+    import tigre_b200 as tigre
+    name, geo, ang, img = case
+    proj = O.ax(img, geo, ang, "Siddon")
+    got = tigre.Atb(proj, geo, ang, btype)
+    ref = O.atb(proj, geo, ang, btype)
+    mx, l2 = G.rel_err(got, ref)
+    assert mx <= TOL and l2 <= TOL, (name, btype, mx, l2)
+
+
+@pytest.mark.parametrize("ptype", ["Siddon", "interpolated"])
+def test_device_api_equals_host_api(case, ptype):
+    torch = _torch()
+    import tigre_b200 as tigre
+    name, geo, ang, img = case
+    host = tigre.Ax(img, geo, ang, ptype)
+    dev = tigre.Ax(torch.from_numpy(img).cuda(), geo, ang, ptype).cpu().numpy()
+    np.testing.assert_array_equal(dev, host)
+
+
+def test_device_atb_equals_host(case):
+    torch = _torch()
+    import tigre_b200 as tigre
+    name, geo, ang, img = case
+    proj = O.ax(img, geo, ang, "Siddon")
+    for bt in ("FDK", "matched"):
+        host = tigre.Atb(proj, geo, ang, bt)
+        dev = tigre.Atb(torch.from_numpy(proj).cuda(), geo, ang, bt).cpu().numpy()
+        np.testing.assert_array_equal(dev, host)
+
+
+def test_siddon_segment_count_matches_oracle():
+    torch = _torch()
+    from tigre_b200 import _native as N, projectors
+    geo, ang = G.c1_geometry(), G.angles(20)
+    img = G.phantom((64, 64, 64))
+    _, cnt = O.ax(img, geo, ang, "Siddon", return_counts=True)
+    plan = N.get_plan(N.checked_geometry(geo, ang), 0)
+    total = projectors.siddon_segments(plan)
+    # the oracle skips zero-length segments at exact edge crossings
+    assert abs(total - int(cnt.sum())) <= 1e-4 * int(cnt.sum()), (total, int(cnt.sum()))
+
+
+def test_angle_subrange_matches_full():
+    torch = _torch()
+    from tigre_b200 import _native as N, projectors
+    geo, ang = G.c1_geometry(), G.angles(40)
+    img = torch.from_numpy(G.phantom((64, 64, 64))).cuda()
+    plan = N.get_plan(N.checked_geometry(geo, ang), 0)
+    full = projectors.ax(img, plan, "Siddon")
+    part = projectors.ax(img, plan, "Siddon", angle_range=(13, 29))
+    torch.testing.assert_close(part, full[13:29], rtol=0, atol=0)
+    bp_full = projectors.atb(full[13:29].contiguous(), plan, "matched", angle_range=(13, 29))
+    ref = O.atb(full.cpu().numpy(), geo, ang, "matched", angle_range=(13, 29))
+    mx, l2 = G.rel_err(bp_full.cpu().numpy(), ref)
+    assert mx <= TOL and l2 <= TOL
+
+
+def test_tv_gradient_and_pocs_match_oracle():
+    torch = _torch()
+    from tigre_b200 import projectors
+    rng = np.random.default_rng(5)
+    img = (G.phantom((24, 31, 29), seed=4) + rng.normal(0, 1e-3, (24, 31, 29))).astype(np.float32)
+    g = projectors.tv_gradient(torch.from_numpy(img).cuda()).cpu().numpy()
+    gref = O.tv_gradient(img)
+    mx, l2 = G.rel_err(g, gref)
+    assert mx <= 1e-4 and l2 <= TOL, (mx, l2)
+    import tigre_b200 as tigre
+    out = tigre.minTV(img, alpha=0.002, maxiter=20)
+    ref = O.pocs_tv(img, 0.002, 20)
+    mx, l2 = G.rel_err(out, ref)
+    assert mx <= TOL and l2 <= TOL, (mx, l2)
+
+
+def test_tv_value_consistent_with_gradient():
+    """Central differences of tv_value reproduce tv_gradient (noisy volume, |grad| >> eps)."""
+    torch = _torch()
+    from tigre_b200 import projectors
+    rng = np.random.default_rng(7)
+    x = torch.from_numpy(rng.normal(0, 1, (6, 7, 8)).astype(np.float32)).cuda()
+    g = projectors.tv_gradient(x).cpu().numpy().astype(np.float64)
+    h = 1e-2
+    idx = [(0, 0, 0), (5, 6, 7), (2, 3, 4), (5, 0, 3), (0, 6, 7)]
+    for (z, y, xx) in idx:
+        xp = x.clone(); xp[z, y, xx] += h
+        xm = x.clone(); xm[z, y, xx] -= h
+        fd = (projectors.tv_value(xp).item() - projectors.tv_value(xm).item()) / (2 * h)
+        assert abs(fd - g[z, y, xx]) <= 2e-3 * max(1.0, abs(g[z, y, xx])), ((z, y, xx), fd, g[z, y, xx])
+
+
+def test_bf16_storage_error_is_small():
+    """Reduced-precision storage: stated error against the FP64 oracle (bound 1e-2)."""
+    torch = _torch()
+    from tigre_b200 import _native as N, projectors
+    geo, ang = G.c1_geometry(), G.angles(50)
+    img = G.phantom((64, 64, 64))
+    plan = N.get_plan(N.checked_geometry(geo, ang), 0)
+    ref = O.ax(img, geo, ang, "Siddon")
+    for dt in (torch.bfloat16, torch.float16):
+        p = projectors.ax(torch.from_numpy(img).cuda().to(dt), plan, "Siddon", out_dtype=torch.float32)
+        mx, l2 = G.rel_err(p.cpu().numpy(), ref)
+        assert l2 <= 1e-2, (dt, mx, l2)
+
+
+def test_adjoint_dot_test_matched():
+    """<Ax, y> vs <x, A^T y> for Siddon + matched; the matched weight is the reference's
+    approximate adjoint, so the gap is reported and bounded loosely (2%)."""
+    torch = _torch()
+    from tigre_b200 import _native as N, projectors
+    geo, ang = G.c1_geometry(), G.angles(60)
+    rng = np.random.default_rng(11)
+    x = torch.from_numpy(rng.random((64, 64, 64), dtype=np.float32)).cuda()
+    y = torch.from_numpy(rng.random((60, 128, 128), dtype=np.float32)).cuda()
+    plan = N.get_plan(N.checked_geometry(geo, ang), 0)
+    ax = projectors.ax(x, plan, "Siddon")
+    aty = projectors.atb(y, plan, "matched")
+    lhs = float((ax.double() * y.double()).sum())
+    rhs = float((x.double() * aty.double()).sum())
+    assert abs(lhs - rhs) / abs(lhs) < 0.02, (lhs, rhs)
+
+
+def test_empty_and_missing_rays():
+    """Views whose rays miss the volume entirely give exact zeros (reference writes 0)."""
+    torch = _torch()
+    import tigre_b200 as tigre
+    geo = G.c1_geometry()
+    geo.offOrigin = np.array((500.0, 0.0, 0.0))    # volume moved 500 mm along z, out of the cone
+    img = G.phantom((64, 64, 64))
+    p = tigre.Ax(img, geo, G.angles(4), "Siddon")
+    assert np.all(p == 0)
+    q = tigre.Ax(img, geo, G.angles(4), "interpolated")
+    assert np.all(q == 0)

@@ -1,0 +1,57 @@
+// C++-linkage shims with the reference's exact signatures (see
+// include/tigre_b200_compat.hpp), forwarding to the extern "C" entry points.
+#include <cstdio>
+
+#include "../../include/tigre_b200_compat.hpp"
+#include "../../include/tigre_b200.h"
+
+static_assert(sizeof(Geometry) == sizeof(TigreGeometry), "Geometry layout must match TigreGeometry");
+
+namespace {
+inline const TigreGeometry* as_c(const Geometry& g) { return reinterpret_cast<const TigreGeometry*>(&g); }
+}  // namespace
+
+int siddon_ray_projection(float* img, Geometry geo, float** result, float const* const angles, int nangles,
+                          const GpuIds& ids) {
+    return tigre_siddon_ray_projection(img, as_c(geo), result, angles, nangles, ids.m_piDeviceIds, ids.m_iCount);
+}
+
+int siddon_ray_projection_parallel(float* img, Geometry geo, float** result, float const* const angles, int nangles,
+                                   const GpuIds& ids) {
+    return tigre_siddon_ray_projection_parallel(img, as_c(geo), result, angles, nangles, ids.m_piDeviceIds,
+                                                ids.m_iCount);
+}
+
+int interpolation_projection(float* img, Geometry geo, float** result, float const* const angles, int nangles,
+                             const GpuIds& ids) {
+    return tigre_interpolation_projection(img, as_c(geo), result, angles, nangles, ids.m_piDeviceIds, ids.m_iCount);
+}
+
+int interpolation_projection_parallel(float* img, Geometry geo, float** result, float const* const angles,
+                                      int nangles, const GpuIds& ids) {
+    return tigre_interpolation_projection_parallel(img, as_c(geo), result, angles, nangles, ids.m_piDeviceIds,
+                                                   ids.m_iCount);
+}
+
+int voxel_backprojection(float* projections, Geometry geo, float* result, float const* const alphas, int nalpha,
+                         const GpuIds& ids) {
+    return tigre_voxel_backprojection(projections, as_c(geo), result, alphas, nalpha, ids.m_piDeviceIds,
+                                      ids.m_iCount);
+}
+
+int voxel_backprojection2(float* projections, Geometry geo, float* result, float const* const alphas, int nalpha,
+                          const GpuIds& ids) {
+    return tigre_voxel_backprojection2(projections, as_c(geo), result, alphas, nalpha, ids.m_piDeviceIds,
+                                       ids.m_iCount);
+}
+
+int voxel_backprojection_parallel(float* projections, Geometry geo, float* result, float const* const alphas,
+                                  int nalpha, const GpuIds& ids) {
+    return tigre_voxel_backprojection_parallel(projections, as_c(geo), result, alphas, nalpha, ids.m_piDeviceIds,
+                                               ids.m_iCount);
+}
+
+void pocs_tv(float* img, float* dst, float alpha, const long* image_size, int maxIter, const GpuIds& ids) {
+    const int rc = tigre_pocs_tv(img, dst, alpha, image_size, maxIter, ids.m_piDeviceIds, ids.m_iCount);
+    if (rc) std::fprintf(stderr, "minimizeTV:POCS_TV: error %d: %s\n", rc, tigre_last_error());
+}

@@ -1,0 +1,98 @@
+// Working layouts of the projectors.
+//
+// The caller's volume is (z, y, x), x fastest.  A warp of rays covers 32
+// neighbouring detector columns; when those columns step mostly along y (view
+// angles near 0 or pi) the rays of the warp sit at 32 consecutive y, so a
+// y-fastest copy (z, x, y) turns their gathers into one or two cache lines per
+// warp load.  make_layout builds either copy, optionally zero-padded
+// (pad_lo/pad_hi voxels per side) so that interpolation needs no bounds tests.
+// pad_projections builds the zero-bordered projection stack of the
+// backprojector (1 pixel before, 2 after, in u and v).
+
+#include "tigre_internal.h"
+
+namespace tigre {
+namespace {
+
+constexpr int TILE = 32;
+
+// layout 0: dst (Z', Y', X') x fastest;  layout 1: dst (Z', X', Y') y fastest.
+// Primed extents are n + pad_lo + pad_hi; source coordinate = dst - pad_lo.
+template <typename T, int LAYOUT>
+__global__ void make_layout_kernel(const T* __restrict__ src, T* __restrict__ dst, int nX, int nY, int nZ, int plo,
+                                   int phi) {
+    __shared__ T tile[TILE][TILE + 1];
+    const int XP = nX + plo + phi, YP = nY + plo + phi;
+    const int zp = blockIdx.z;
+    const int z = zp - plo;
+    const bool zin = z >= 0 && z < nZ;
+    // tile origin in (yp, xp)
+    const int xp0 = blockIdx.x * TILE, yp0 = blockIdx.y * TILE;
+    const size_t plane_src = (size_t)nX * nY;
+    // load: threads along x for coalesced reads
+    for (int j = threadIdx.y; j < TILE; j += blockDim.y) {
+        const int yp = yp0 + j, xp = xp0 + threadIdx.x;
+        const int y = yp - plo, x = xp - plo;
+        T v = from_f32<T>(0.f);
+        if (zin && x >= 0 && x < nX && y >= 0 && y < nY) v = src[(size_t)z * plane_src + (size_t)y * nX + x];
+        tile[j][threadIdx.x] = v;
+    }
+    __syncthreads();
+    if (LAYOUT == 0) {
+        for (int j = threadIdx.y; j < TILE; j += blockDim.y) {
+            const int yp = yp0 + j, xp = xp0 + threadIdx.x;
+            if (yp < YP && xp < XP) dst[((size_t)zp * YP + yp) * XP + xp] = tile[j][threadIdx.x];
+        }
+    } else {
+        // write transposed: threads along y
+        for (int j = threadIdx.y; j < TILE; j += blockDim.y) {
+            const int xp = xp0 + j, yp = yp0 + threadIdx.x;
+            if (yp < YP && xp < XP) dst[((size_t)zp * XP + xp) * YP + yp] = tile[threadIdx.x][j];
+        }
+    }
+}
+
+template <typename T>
+__global__ void pad_projections_kernel(const T* __restrict__ src, T* __restrict__ dst, int nV, int nU, long total) {
+    const long pitch = bp_pitch(nU), rows = bp_rows(nV);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const long a = i / (pitch * rows);
+        const long rem = i - a * pitch * rows;
+        const int r = (int)(rem / pitch), c = (int)(rem - (long)r * pitch);
+        const int v = r - 1, u = c - 1;
+        T val = from_f32<T>(0.f);
+        if (v >= 0 && v < nV && u >= 0 && u < nU) val = src[(a * nV + v) * (long)nU + u];
+        dst[i] = val;
+    }
+}
+
+}  // namespace
+
+int launch_make_layout(const void* src, int dtype, void* dst, int nX, int nY, int nZ, int layout, int pad_lo,
+                       int pad_hi, cudaStream_t st) {
+    const int p = pad_lo + pad_hi;
+    dim3 block(TILE, 8);
+    dim3 grid((nX + p + TILE - 1) / TILE, (nY + p + TILE - 1) / TILE, nZ + p);
+    TIGRE_DISPATCH_DTYPE(dtype, T, {
+        if (layout == 0)
+            make_layout_kernel<T, 0><<<grid, block, 0, st>>>((const T*)src, (T*)dst, nX, nY, nZ, pad_lo, pad_hi);
+        else
+            make_layout_kernel<T, 1><<<grid, block, 0, st>>>((const T*)src, (T*)dst, nX, nY, nZ, pad_lo, pad_hi);
+    });
+    TIGRE_CUDA(cudaGetLastError());
+    return TIGRE_SUCCESS;
+}
+
+int launch_pad_projections(const void* src, int dtype, void* dst, int nA, int nV, int nU, cudaStream_t st) {
+    const long total = (long)nA * bp_rows(nV) * bp_pitch(nU);
+    const int block = 256;
+    const long want = (total + block - 1) / block;
+    const int grid = (int)std::min<long>(want, 148L * 32);
+    TIGRE_DISPATCH_DTYPE(dtype, T, {
+        pad_projections_kernel<T><<<grid, block, 0, st>>>((const T*)src, (T*)dst, nV, nU, total);
+    });
+    TIGRE_CUDA(cudaGetLastError());
+    return TIGRE_SUCCESS;
+}
+
+}  // namespace tigre

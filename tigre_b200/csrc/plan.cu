@@ -1,0 +1,288 @@
+// Plan creation: FP64 per-angle frames of the cone-beam geometry, uploaded
+// once; error state; the stream-ordered scratch arena.
+//
+// The frame formulas are the reference's (they define the geometry and must
+// agree with it); each block cites the function it restates:
+//   Siddon frame      computeDeltas_Siddon, Common/CUDA/Siddon_projection.cu:666-763
+//   rotations         rollPitchYaw, Common/CUDA/projection.cpp:18-35;
+//                     eulerZYZ, Siddon_projection.cu:801-820
+//   interpolated      computeDeltas + maxdistanceCuboid, ray_interpolated_projection.cu:632-768
+//   backprojection    computeDeltasCube + eulerZYZT + rollPitchYawT,
+//                     Common/CUDA/voxel_backprojection.cu:762-898
+// The reference evaluates most of them in float; here everything is double.
+
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <mutex>
+
+#include "tigre_internal.h"
+
+namespace tigre {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg) {
+    set_error(msg);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return TIGRE_ERR_CUDA;
+}
+
+namespace {
+
+struct Vec { double x, y, z; };
+
+struct Rot3 {
+    double m[3][3];
+    Vec apply(const Vec& p) const {
+        return {m[0][0] * p.x + m[0][1] * p.y + m[0][2] * p.z, m[1][0] * p.x + m[1][1] * p.y + m[1][2] * p.z,
+                m[2][0] * p.x + m[2][1] * p.y + m[2][2] * p.z};
+    }
+    Rot3 transposed() const {
+        Rot3 t;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) t.m[i][j] = m[j][i];
+        return t;
+    }
+};
+
+// detector roll/pitch/yaw (projection.cpp:18-35)
+Rot3 detector_rotation(double roll, double pitch, double yaw) {
+    const double cr = std::cos(roll), sr = std::sin(roll), cp = std::cos(pitch), sp = std::sin(pitch);
+    const double cy = std::cos(yaw), sy = std::sin(yaw);
+    Rot3 r;
+    r.m[0][0] = cr * cp; r.m[0][1] = cr * sp * sy - sr * cy; r.m[0][2] = cr * sp * cy + sr * sy;
+    r.m[1][0] = sr * cp; r.m[1][1] = sr * sp * sy + cr * cy; r.m[1][2] = sr * sp * cy - cr * sy;
+    r.m[2][0] = -sp;     r.m[2][1] = cp * sy;                r.m[2][2] = cp * cy;
+    return r;
+}
+
+// ZYZ Euler rotation (Siddon_projection.cu:801-820); eulerZYZT of the
+// backprojectors is the same matrix at negated angles.
+Rot3 euler_zyz(double a, double t, double p) {
+    const double ca = std::cos(a), sa = std::sin(a), ct = std::cos(t), st = std::sin(t);
+    const double cp = std::cos(p), sp = std::sin(p);
+    Rot3 r;
+    r.m[0][0] = ca * ct * cp - sa * sp; r.m[0][1] = -ca * ct * sp - sa * cp; r.m[0][2] = ca * st;
+    r.m[1][0] = sa * ct * cp + ca * sp; r.m[1][1] = -sa * ct * sp + ca * cp; r.m[1][2] = sa * st;
+    r.m[2][0] = -st * cp;               r.m[2][1] = st * sp;                 r.m[2][2] = ct;
+    return r;
+}
+
+// eulerZYZT (voxel_backprojection.cu:762-785): entries arranged with psi/alpha swapped
+Rot3 euler_zyz_T(double a, double t, double p) {
+    const double ca = std::cos(a), sa = std::sin(a), ct = std::cos(t), st = std::sin(t);
+    const double cp = std::cos(p), sp = std::sin(p);
+    Rot3 r;
+    r.m[0][0] = cp * ct * ca - sp * sa; r.m[0][1] = -cp * ct * sa - sp * ca; r.m[0][2] = cp * st;
+    r.m[1][0] = sp * ct * ca + cp * sa; r.m[1][1] = -sp * ct * sa + cp * ca; r.m[1][2] = sp * st;
+    r.m[2][0] = -st * ca;               r.m[2][1] = st * sa;                 r.m[2][2] = ct;
+    return r;
+}
+
+inline double at(const float* a, int i) { return a ? (double)a[i] : 0.0; }
+
+}  // namespace
+
+int compute_frames(const TigreGeometry* g, const float* angles, int nangles, TigrePlan* plan) {
+    TIGRE_CHECK(g != nullptr && angles != nullptr, "null geometry or angles");
+    TIGRE_CHECK(nangles > 0, "nangles must be positive");
+    TIGRE_CHECK(g->nVoxelX > 0 && g->nVoxelY > 0 && g->nVoxelZ > 0, "nVoxel must be positive");
+    TIGRE_CHECK(g->nDetecU > 0 && g->nDetecV > 0, "nDetector must be positive");
+    TIGRE_CHECK(g->DSO && g->DSD, "DSO/DSD arrays are required");
+    TIGRE_CHECK((double)g->nVoxelX * g->nVoxelY * g->nVoxelZ < 2147483647.0 * 0.99,
+                "volume larger than 2^31 voxels is not supported");
+    Dims& d = plan->d;
+    d.nX = g->nVoxelX; d.nY = g->nVoxelY; d.nZ = g->nVoxelZ;
+    d.nU = g->nDetecU; d.nV = g->nDetecV; d.nA = nangles;
+    d.sVX = g->sVoxelX; d.sVY = g->sVoxelY; d.sVZ = g->sVoxelZ;
+    d.dVX = g->dVoxelX; d.dVY = g->dVoxelY; d.dVZ = g->dVoxelZ;
+    d.sDU = g->sDetecU; d.sDV = g->sDetecV; d.dDU = g->dDetecU; d.dDV = g->dDetecV;
+    d.accuracy = g->accuracy;
+    TIGRE_CHECK(d.dVX > 0 && d.dVY > 0 && d.dVZ > 0 && d.dDU > 0 && d.dDV > 0, "voxel/pixel sizes must be positive");
+    TIGRE_CHECK(d.accuracy > 0, "accuracy must be positive");
+
+    plan->h_siddon.resize(nangles);
+    plan->h_interp.resize(nangles);
+    plan->h_bp.resize(nangles);
+    bool axial = true;
+    for (int i = 0; i < nangles; ++i) {
+        const double al = angles[3 * i], th = angles[3 * i + 1], ps = angles[3 * i + 2];
+        const double dso = g->DSO[i], dsd = g->DSD[i];
+        const double offx = at(g->offOrigX, i), offy = at(g->offOrigY, i), offz = at(g->offOrigZ, i);
+        const double offu = at(g->offDetecU, i), offv = at(g->offDetecV, i);
+        const double cor = at(g->COR, i);
+        const Rot3 rd = detector_rotation(at(g->dRoll, i), at(g->dPitch, i), at(g->dYaw, i));
+        const Rot3 re = euler_zyz(al, th, ps);
+
+        // ---- Siddon frame (computeDeltas_Siddon) ----
+        Vec S{dso, 0.0, 0.0};
+        Vec P{0.0, d.dDU * (-(double)d.nU / 2.0 + 0.5), d.dDV * ((double)d.nV / 2.0 - 0.5)};
+        Vec Pu{0.0, d.dDU, 0.0}, Pv{0.0, 0.0, -d.dDV};
+        P = rd.apply(P); Pu = rd.apply(Pu); Pv = rd.apply(Pv);
+        P.x -= (dsd - dso);
+        P.y += offu; P.z += offv;
+        P = re.apply(P); Pu = re.apply(Pu); Pv = re.apply(Pv); S = re.apply(S);
+        const double cx = -offx + d.sVX / 2, cy = -offy + d.sVY / 2, cz = -offz + d.sVZ / 2;
+        P = {(P.x + cx) / d.dVX, (P.y + cy) / d.dVY, (P.z + cz) / d.dVZ};
+        S = {(S.x + cx) / d.dVX, (S.y + cy) / d.dVY, (S.z + cz) / d.dVZ};
+        Pu = {Pu.x / d.dVX, Pu.y / d.dVY, Pu.z / d.dVZ};
+        Pv = {Pv.x / d.dVX, Pv.y / d.dVY, Pv.z / d.dVZ};
+        const double corx = -cor * std::sin(al) / d.dVX, cory = cor * std::cos(al) / d.dVY;
+        P.x += corx; P.y += cory; S.x += corx; S.y += cory;
+        FrameSiddon& fs = plan->h_siddon[i];
+        fs.o[0] = P.x; fs.o[1] = P.y; fs.o[2] = P.z;
+        fs.du[0] = Pu.x; fs.du[1] = Pu.y; fs.du[2] = Pu.z;
+        fs.dv[0] = Pv.x; fs.dv[1] = Pv.y; fs.dv[2] = Pv.z;
+        fs.s[0] = S.x; fs.s[1] = S.y; fs.s[2] = S.z;
+        // neighbouring detector columns move mostly along y -> y-fastest working copy
+        fs.layout = std::fabs(Pu.y) >= std::fabs(Pu.x) ? 1 : 0;
+        fs.pad_ = 0;
+
+        // ---- interpolated frame: voxel centres at integers (computeDeltas) ----
+        FrameInterp& fi = plan->h_interp[i];
+        for (int k = 0; k < 3; ++k) {
+            fi.o[k] = fs.o[k] - 0.5; fi.du[k] = fs.du[k]; fi.dv[k] = fs.dv[k]; fi.s[k] = fs.s[k] - 0.5;
+        }
+        fi.layout = fs.layout;
+        fi.pad_ = 0;
+        {
+            // maxdistanceCuboid: note the C integer division nVoxel/2 of the reference
+            const double mx = (double)(d.nX / 2) + std::fabs(offx) / d.dVX;
+            const double my = (double)(d.nY / 2) + std::fabs(offy) / d.dVY;
+            const double mz = (double)(d.nZ / 2) + std::fabs(offz) / d.dVZ;
+            const double a = dso / d.dVX, b = dso / d.dVY;
+            double md;
+            if (th == 0.0 && ps == 0.0) {
+                const double sa = std::sin(al), ca = std::cos(al);
+                md = a * b / std::sqrt(a * a * sa * sa + b * b * ca * ca) - std::sqrt(mx * mx + my * my);
+            } else {
+                md = dso / std::max(std::max(d.dVX, d.dVY), d.dVZ) - std::sqrt(mx * mx + my * my + mz * mz);
+            }
+            const double crop = std::floor(std::max(md, 0.0));
+            fi.first_sample = std::floor(crop / d.accuracy);
+            // the reference selects the spherical cap per launch of 9 angles
+            const int b0 = (i / 9) * 9, b1 = std::min(b0 + 9, nangles);
+            double sph = 0.0;
+            for (int k = b0; k < b1; ++k) sph += std::fabs(angles[3 * k + 1]) + std::fabs(angles[3 * k + 2]);
+            const double dmin = sph != 0.0 ? std::min(std::min(d.dVX, d.dVY), d.dVZ) : std::min(d.dVX, d.dVY);
+            fi.cap = (2.0 * dso / dmin + crop) / d.accuracy;
+        }
+
+        // ---- backprojection frame (computeDeltasCube, angles negated) ----
+        {
+            const Rot3 rt = euler_zyz_T(-al, -th, -ps);
+            const Rot3 rdt = detector_rotation(at(g->dRoll, i), at(g->dPitch, i), at(g->dYaw, i)).transposed();
+            Vec Q{-(d.sVX / 2 - d.dVX / 2) + offx, -(d.sVY / 2 - d.dVY / 2) + offy, -(d.sVZ / 2 - d.dVZ / 2) + offz};
+            Vec pts[4] = {Q, {Q.x + d.dVX, Q.y, Q.z}, {Q.x, Q.y + d.dVY, Q.z}, {Q.x, Q.y, Q.z + d.dVZ}};
+            const double off = dsd - dso;
+            for (Vec& p : pts) {
+                p = rt.apply(p);
+                p.z -= offv; p.y -= offu;
+                p.x += off;
+                p = rdt.apply(p);
+                p.x -= off;
+                p.z /= d.dDV; p.y /= d.dDU;
+            }
+            Vec src{dsd, -offu, -offv};
+            src = rdt.apply(src);
+            src.x -= off;
+            src.z /= d.dDV; src.y /= d.dDU;
+            FrameBP& fb = plan->h_bp[i];
+            fb.o[0] = pts[0].x; fb.o[1] = pts[0].y; fb.o[2] = pts[0].z;
+            const Vec* q = pts;
+            fb.dx[0] = q[1].x - q[0].x; fb.dx[1] = q[1].y - q[0].y; fb.dx[2] = q[1].z - q[0].z;
+            fb.dy[0] = q[2].x - q[0].x; fb.dy[1] = q[2].y - q[0].y; fb.dy[2] = q[2].z - q[0].z;
+            fb.dz[0] = q[3].x - q[0].x; fb.dz[1] = q[3].y - q[0].y; fb.dz[2] = q[3].z - q[0].z;
+            fb.s[0] = src.x; fb.s[1] = src.y; fb.s[2] = src.z;
+            fb.sina = (float)std::sin(-al);
+            fb.cosa = (float)std::cos(-al);
+            fb.cor = (float)cor; fb.dsd = (float)dsd; fb.dso = (float)dso;
+            fb.offx = (float)offx; fb.offy = (float)offy; fb.offz = (float)offz;
+            fb.offu = (float)offu; fb.offv = (float)offv;
+            if (std::fabs(fb.dz[0]) > 1e-12 * d.dVZ || std::fabs(fb.dz[1]) > 1e-12 * d.dVZ) axial = false;
+        }
+    }
+    plan->axial = axial;
+    return TIGRE_SUCCESS;
+}
+
+void* plan_scratch(TigrePlan* plan, size_t bytes, cudaStream_t st, int* rc) {
+    *rc = TIGRE_SUCCESS;
+    if (bytes <= plan->scratch_bytes) return plan->scratch;
+    if (plan->scratch) {
+        cudaError_t e = cudaFreeAsync(plan->scratch, st);
+        if (e != cudaSuccess) { *rc = cuda_fail(e, "cudaFreeAsync(scratch)"); return nullptr; }
+        plan->scratch = nullptr;
+        plan->scratch_bytes = 0;
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, bytes, st);
+    if (e != cudaSuccess) { *rc = cuda_fail(e, "cudaMallocAsync(scratch)"); return nullptr; }
+    plan->scratch = p;
+    plan->scratch_bytes = bytes;
+    return p;
+}
+
+}  // namespace tigre
+
+using namespace tigre;
+
+extern "C" {
+
+const char* tigre_last_error(void) { return g_last_error.c_str(); }
+
+int tigre_version(void) { return 100; }
+
+int tigre_plan_create(const TigreGeometry* geo, const float* angles, int nangles, int device, TigrePlan** out) {
+    if (!out) return fail(TIGRE_ERR_BAD_ASSERT, "null output plan pointer");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return fail(TIGRE_ERR_NO_CAPABLE_DEVICES, "no CUDA device available");
+    if (device < 0 || device >= ndev) return fail(TIGRE_ERR_BAD_ASSERT, "device id out of range");
+    TigrePlan* p = new TigrePlan();
+    p->device = device;
+    int rc = compute_frames(geo, angles, nangles, p);
+    if (rc) { delete p; return rc; }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    const size_t ns = sizeof(FrameSiddon) * nangles, ni = sizeof(FrameInterp) * nangles, nb = sizeof(FrameBP) * nangles;
+    e = cudaMalloc(&p->d_siddon, ns);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_interp, ni);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_bp, nb);
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_siddon, p->h_siddon.data(), ns, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_interp, p->h_interp.data(), ni, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_bp, p->h_bp.data(), nb, cudaMemcpyHostToDevice);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        tigre_plan_destroy(p);
+        return cuda_fail(e, "plan upload");
+    }
+    *out = p;
+    return TIGRE_SUCCESS;
+}
+
+void tigre_plan_destroy(TigrePlan* p) {
+    if (!p) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(p->device);
+    if (p->scratch) { cudaDeviceSynchronize(); cudaFree(p->scratch); }
+    cudaFree(p->d_siddon);
+    cudaFree(p->d_interp);
+    cudaFree(p->d_bp);
+    cudaSetDevice(prev);
+    delete p;
+}
+
+long long tigre_plan_scratch_bytes(const TigrePlan* p) { return p ? (long long)p->scratch_bytes : 0; }
+
+}  // extern "C"

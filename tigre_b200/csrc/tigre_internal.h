@@ -1,0 +1,140 @@
+// Internal declarations of libtigre_b200: plan layout, per-angle frames,
+// kernel launchers.  Not part of the public ABI (see include/tigre_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/tigre_b200.h"
+
+namespace tigre {
+
+// ---------------------------------------------------------------- errors --
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define TIGRE_CUDA(call)                                     \
+    do {                                                     \
+        cudaError_t e__ = (call);                            \
+        if (e__ != cudaSuccess) return cuda_fail(e__, #call); \
+    } while (0)
+
+#define TIGRE_CHECK(cond, msg)                                    \
+    do {                                                          \
+        if (!(cond)) return fail(TIGRE_ERR_BAD_ASSERT, (msg));    \
+    } while (0)
+
+inline size_t dtype_size(int dt) { return dt == TIGRE_F32 ? 4 : 2; }
+inline bool dtype_ok(int dt) { return dt == TIGRE_F32 || dt == TIGRE_BF16 || dt == TIGRE_F16; }
+
+// ------------------------------------------------------- per-angle frames --
+// All frames are computed on the host in FP64 from the float32 geometry, once
+// per plan, with the reference's formulas (cited in geometry.cpp).
+
+// Siddon: voxel-index units, volume corner at the origin (voxel i spans [i, i+1)).
+struct FrameSiddon {
+    double o[3];    // detector pixel (u=0, pixelV=0), pixelV = nV-1-v
+    double du[3];   // step per u
+    double dv[3];   // step per pixelV
+    double s[3];    // source
+    int layout;     // 0: x-fastest working layout, 1: y-fastest (transposed)
+    int pad_;
+};
+
+// Interpolated: voxel-centre units (voxel i centred at i).
+struct FrameInterp {
+    double o[3], du[3], dv[3], s[3];
+    double first_sample;   // floor(cropdist/accuracy), ray_interpolated_projection.cu:193
+    double cap;            // sample-count cap (:179-189); +inf when it cannot bind
+    int layout;
+    int pad_;
+};
+
+// Backprojection: detector-pixel units in y/z, mm in x (computeDeltasCube).
+struct FrameBP {
+    double o[3], dx[3], dy[3], dz[3], s[3];
+    float sina, cosa;   // of the negated alpha (voxel_backprojection.cu:510-515)
+    float cor, dsd, dso;
+    float offx, offy, offz;   // offOrig
+    float offu, offv;         // offDetec
+};
+
+struct Plan;
+
+// ----------------------------------------------------------------- plan ---
+struct Dims {
+    int nX, nY, nZ;      // volume
+    int nU, nV;          // detector
+    int nA;              // angles in the plan
+    double sVX, sVY, sVZ, dVX, dVY, dVZ;
+    double sDU, sDV, dDU, dDV;
+    double accuracy;
+};
+
+}  // namespace tigre
+
+struct TigrePlan {
+    int device = 0;
+    tigre::Dims d{};
+    std::vector<tigre::FrameSiddon> h_siddon;
+    std::vector<tigre::FrameInterp> h_interp;
+    std::vector<tigre::FrameBP> h_bp;
+    tigre::FrameSiddon* d_siddon = nullptr;
+    tigre::FrameInterp* d_interp = nullptr;
+    tigre::FrameBP* d_bp = nullptr;
+    bool axial = false;          // every BP frame has dz.x == dz.y == 0 (u constant along z)
+    // growable stream-ordered scratch arena
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+};
+
+namespace tigre {
+
+int compute_frames(const TigreGeometry* geo, const float* angles, int nangles, TigrePlan* plan);
+void* plan_scratch(TigrePlan* plan, size_t bytes, cudaStream_t st, int* rc);
+
+// ------------------------------------------------------------ launchers ---
+int launch_make_layout(const void* src, int dtype, void* dst, int nX, int nY, int nZ, int layout, int pad_lo,
+                       int pad_hi, cudaStream_t st);
+int launch_pad_projections(const void* src, int dtype, void* dst, int nA, int nV, int nU, cudaStream_t st);
+
+int launch_siddon(TigrePlan* p, const void* vol_x, const void* vol_y, int vdt, void* proj, int pdt, int a0, int a1,
+                  cudaStream_t st);
+int launch_siddon_count(TigrePlan* p, int a0, int a1, unsigned long long* d_total, cudaStream_t st);
+int launch_interp(TigrePlan* p, const void* vol_x, const void* vol_y, int vdt, void* proj, int pdt, int a0, int a1,
+                  cudaStream_t st);
+int launch_backproject(TigrePlan* p, const void* proj_pad, int pdt, void* vol, int vdt, int matched, int a0, int a1,
+                       cudaStream_t st);
+
+// padded projection pitch and row count used by the backprojector
+__host__ __device__ inline long bp_pitch(int nU) { return (long)nU + 3; }
+__host__ __device__ inline long bp_rows(int nV) { return (long)nV + 3; }
+
+// ------------------------------------------------------ dtype helpers -----
+template <typename T> __device__ __forceinline__ float to_f32(T v);
+template <> __device__ __forceinline__ float to_f32<float>(float v) { return v; }
+template <> __device__ __forceinline__ float to_f32<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <> __device__ __forceinline__ float to_f32<__half>(__half v) { return __half2float(v); }
+
+template <typename T> __device__ __forceinline__ T from_f32(float v);
+template <> __device__ __forceinline__ float from_f32<float>(float v) { return v; }
+template <> __device__ __forceinline__ __nv_bfloat16 from_f32<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+template <> __device__ __forceinline__ __half from_f32<__half>(float v) { return __float2half_rn(v); }
+
+template <typename T> __device__ __forceinline__ float ldg_f(const T* p) { return to_f32<T>(__ldg(p)); }
+
+// dispatch a templated functor on a storage dtype
+#define TIGRE_DISPATCH_DTYPE(dt, T, ...)                       \
+    switch (dt) {                                              \
+        case TIGRE_F32: { using T = float; __VA_ARGS__; break; }          \
+        case TIGRE_BF16: { using T = __nv_bfloat16; __VA_ARGS__; break; } \
+        case TIGRE_F16: { using T = __half; __VA_ARGS__; break; }         \
+        default: return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype");  \
+    }
+
+}  // namespace tigre

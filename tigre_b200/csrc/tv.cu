@@ -1,0 +1,209 @@
+// POCS total-variation descent, sm_100a.
+//
+// One step of pocs_tv (Common/CUDA/GD_TV.cu:440-597) is
+//     g = grad TV(f)                                  (gradientTV, :117-143)
+//     f <- f - alpha * g / sqrt(sum(g^2) + 1e-7)      (:556-597)
+// The reference runs gradientTV, a device copy, two reduction kernels, a host
+// synchronisation and three element-wise kernels per step (~48 B/voxel).
+// Here a step is two passes and no host round trip (~12 B/voxel):
+//   pass 1  tv_norm_kernel    stencil -> g, sum g^2 (FP64, one atomic per block)
+//   pass 2  tv_update_kernel  stencil again -> g, writes f - alpha g / |g|,
+//                             reading |g|^2 from device memory (ping-pong buffers)
+// g is recomputed rather than stored: the stencil is cheap, the bytes are not.
+//
+// Boundary rule of the single-device reference call: the image sits between
+// zero slices in z (its zeroed halo buffer, GD_TV.cu:380-393 and 447-461);
+// along x and y a difference whose neighbour is outside is 0 (gradient(), :91-115),
+// and the terms of neighbours beyond the last x / y index vanish.
+
+#include <cmath>
+
+#include "tigre_internal.h"
+
+namespace tigre {
+namespace {
+
+struct TVDims {
+    int nx, ny, nz;
+};
+
+__device__ __forceinline__ float fget(const float* __restrict__ f, const TVDims& d, int x, int y, int z) {
+    return (z >= 0 && z < d.nz) ? __ldg(f + ((size_t)z * d.ny + y) * d.nx + x) : 0.f;
+}
+
+// dftv of GD_TV.cu:135-140 at (x,y,z); eps 1e-8 as the reference.
+__device__ __forceinline__ float tv_grad_at(const float* __restrict__ f, const TVDims& d, int x, int y, int z) {
+    const float eps = 1e-8f;
+    const float c = fget(f, d, x, y, z);
+    const float cxm = x > 0 ? fget(f, d, x - 1, y, z) : 0.f;
+    const float cym = y > 0 ? fget(f, d, x, y - 1, z) : 0.f;
+    const float czm = fget(f, d, x, y, z - 1);
+    // backward differences at the voxel itself
+    const float d0 = c - czm;
+    const float d1 = y > 0 ? c - cym : 0.f;
+    const float d2 = x > 0 ? c - cxm : 0.f;
+    float g = (d0 + d1 + d2) / (sqrtf(d0 * d0 + d1 * d1 + d2 * d2) + eps);
+    if (x + 1 < d.nx) {   // neighbour (x+1): its x difference involves f(x)
+        const float n = fget(f, d, x + 1, y, z);
+        const float e0 = n - fget(f, d, x + 1, y, z - 1);
+        const float e1 = y > 0 ? n - fget(f, d, x + 1, y - 1, z) : 0.f;
+        const float e2 = n - c;
+        g -= e2 / (sqrtf(e0 * e0 + e1 * e1 + e2 * e2) + eps);
+    }
+    if (y + 1 < d.ny) {
+        const float n = fget(f, d, x, y + 1, z);
+        const float e0 = n - fget(f, d, x, y + 1, z - 1);
+        const float e1 = n - c;
+        const float e2 = x > 0 ? n - fget(f, d, x - 1, y + 1, z) : 0.f;
+        g -= e1 / (sqrtf(e0 * e0 + e1 * e1 + e2 * e2) + eps);
+    }
+    {   // neighbour (z+1); above the last slice it is the zero halo slice
+        const float n = fget(f, d, x, y, z + 1);
+        const bool inside = z + 1 < d.nz;
+        const float e0 = n - c;
+        const float e1 = (inside && y > 0) ? n - fget(f, d, x, y - 1, z + 1) : 0.f;
+        const float e2 = (inside && x > 0) ? n - fget(f, d, x - 1, y, z + 1) : 0.f;
+        g -= e0 / (sqrtf(e0 * e0 + e1 * e1 + e2 * e2) + eps);
+    }
+    return g;
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    v = 0.0;
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        v = lane < nw ? red[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+// grid-stride over voxels, x fastest
+__global__ void __launch_bounds__(256) tv_norm_kernel(const float* __restrict__ f, TVDims d, double* __restrict__ out) {
+    const size_t n = (size_t)d.nx * d.ny * d.nz;
+    double s = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % d.nx);
+        const size_t r = i / d.nx;
+        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
+        const float g = tv_grad_at(f, d, x, y, z);
+        s += (double)g * (double)g;
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0) atomicAdd(out, s);
+}
+
+__global__ void __launch_bounds__(256) tv_update_kernel(const float* __restrict__ f, float* __restrict__ o, TVDims d,
+                                                        const double* __restrict__ sumsq, float alpha) {
+    const size_t n = (size_t)d.nx * d.ny * d.nz;
+    // reference: |g| = sqrt(sum + 1e-7), then g/|g| * alpha (GD_TV.cu:561-580)
+    const float scale = (float)((double)alpha / sqrt(*sumsq + 1e-7));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % d.nx);
+        const size_t r = i / d.nx;
+        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
+        const float g = tv_grad_at(f, d, x, y, z);
+        o[i] = fmaf(-scale, g, __ldg(f + i));
+    }
+}
+
+__global__ void __launch_bounds__(256) tv_grad_kernel(const float* __restrict__ f, float* __restrict__ o, TVDims d) {
+    const size_t n = (size_t)d.nx * d.ny * d.nz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % d.nx);
+        const size_t r = i / d.nx;
+        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
+        o[i] = tv_grad_at(f, d, x, y, z);
+    }
+}
+
+// sum_i |grad f_i| over the voxels and the zero halo slice above the last one
+// (whose gradient norm is |f(x,y,nz-1)|); its derivative is tv_grad_at.
+__global__ void __launch_bounds__(256) tv_value_kernel(const float* __restrict__ f, TVDims d, double* __restrict__ out) {
+    const size_t n = (size_t)d.nx * d.ny * (d.nz + 1);
+    double s = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % d.nx);
+        const size_t r = i / d.nx;
+        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
+        if (z == d.nz) {
+            s += fabs((double)fget(f, d, x, y, z - 1));
+            continue;
+        }
+        const float c = fget(f, d, x, y, z);
+        const float d0 = c - fget(f, d, x, y, z - 1);
+        const float d1 = y > 0 ? c - fget(f, d, x, y - 1, z) : 0.f;
+        const float d2 = x > 0 ? c - fget(f, d, x - 1, y, z) : 0.f;
+        s += sqrt((double)d0 * d0 + (double)d1 * d1 + (double)d2 * d2);
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0) atomicAdd(out, s);
+}
+
+int grid_for(size_t n) {
+    const size_t want = (n + 255) / 256;
+    return (int)std::min<size_t>(want, 148 * 16);
+}
+
+}  // namespace
+}  // namespace tigre
+
+using namespace tigre;
+
+extern "C" {
+
+int tigre_tv_gradient(const void* d_img, int dtype, float* d_grad, long nx, long ny, long nz, void* stream) {
+    if (dtype != TIGRE_F32) return fail(TIGRE_ERR_BAD_ASSERT, "TV kernels take float32 volumes");
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !d_img || !d_grad) return fail(TIGRE_ERR_BAD_ASSERT, "bad TV arguments");
+    TVDims d{(int)nx, (int)ny, (int)nz};
+    const size_t n = (size_t)nx * ny * nz;
+    tv_grad_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const float*)d_img, d_grad, d);
+    TIGRE_CUDA(cudaGetLastError());
+    return TIGRE_SUCCESS;
+}
+
+int tigre_tv_value(const void* d_img, int dtype, long nx, long ny, long nz, double* d_out, void* stream) {
+    if (dtype != TIGRE_F32) return fail(TIGRE_ERR_BAD_ASSERT, "TV kernels take float32 volumes");
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !d_img || !d_out) return fail(TIGRE_ERR_BAD_ASSERT, "bad TV arguments");
+    TVDims d{(int)nx, (int)ny, (int)nz};
+    const size_t n = (size_t)nx * ny * (nz + 1);
+    tv_value_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const float*)d_img, d, d_out);
+    TIGRE_CUDA(cudaGetLastError());
+    return TIGRE_SUCCESS;
+}
+
+// In-place POCS-TV.  d_work: nx*ny*nz floats of caller scratch; 8 bytes of
+// reduction scratch are taken from the stream-ordered allocator.
+int tigre_tv_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha, int max_iter, float* d_work,
+                  void* stream) {
+    if (dtype != TIGRE_F32) return fail(TIGRE_ERR_BAD_ASSERT, "TV kernels take float32 volumes");
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !d_img || !d_work || max_iter < 0)
+        return fail(TIGRE_ERR_BAD_ASSERT, "bad TV arguments");
+    if ((double)nx * ny * nz >= 2147483647.0) return fail(TIGRE_ERR_BAD_ASSERT, "volume too large");
+    cudaStream_t st = (cudaStream_t)stream;
+    TVDims d{(int)nx, (int)ny, (int)nz};
+    const size_t n = (size_t)nx * ny * nz;
+    double* sums = nullptr;
+    TIGRE_CUDA(cudaMallocAsync(&sums, sizeof(double) * (size_t)std::max(max_iter, 1), st));
+    TIGRE_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)std::max(max_iter, 1), st));
+    float* cur = (float*)d_img;
+    float* nxt = d_work;
+    for (int it = 0; it < max_iter; ++it) {
+        tv_norm_kernel<<<grid_for(n), 256, 0, st>>>(cur, d, sums + it);
+        tv_update_kernel<<<grid_for(n), 256, 0, st>>>(cur, nxt, d, sums + it, alpha);
+        std::swap(cur, nxt);
+    }
+    if (cur != (float*)d_img) TIGRE_CUDA(cudaMemcpyAsync(d_img, cur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    TIGRE_CUDA(cudaFreeAsync(sums, st));
+    TIGRE_CUDA(cudaGetLastError());
+    return TIGRE_SUCCESS;
+}
+
+}  // extern "C"
