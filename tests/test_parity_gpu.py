@@ -125,15 +125,16 @@ def test_tv_value_consistent_with_gradient():
     torch = _torch()
     from tigre_b200 import projectors
     rng = np.random.default_rng(7)
-    x = torch.from_numpy(rng.normal(0, 1, (6, 7, 8)).astype(np.float32)).cuda()
+    # offset keeps the zero-halo terms |f| away from their kink at 0
+    x = torch.from_numpy((rng.normal(0, 1, (6, 7, 8)) + 4.0).astype(np.float32)).cuda()
     g = projectors.tv_gradient(x).cpu().numpy().astype(np.float64)
-    h = 1e-2
+    h = 1e-3
     idx = [(0, 0, 0), (5, 6, 7), (2, 3, 4), (5, 0, 3), (0, 6, 7)]
     for (z, y, xx) in idx:
         xp = x.clone(); xp[z, y, xx] += h
         xm = x.clone(); xm[z, y, xx] -= h
         fd = (projectors.tv_value(xp).item() - projectors.tv_value(xm).item()) / (2 * h)
-        assert abs(fd - g[z, y, xx]) <= 2e-3 * max(1.0, abs(g[z, y, xx])), ((z, y, xx), fd, g[z, y, xx])
+        assert abs(fd - g[z, y, xx]) <= 5e-3 * max(1.0, abs(g[z, y, xx])), ((z, y, xx), fd, g[z, y, xx])
 
 
 def test_bf16_storage_error_is_small():
