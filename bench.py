@@ -37,13 +37,28 @@ sys.path.insert(0, ROOT)
 
 NV, NU, NA = 768, 1024, 720
 NVOX = (512, 512, 512)
+DDET, SVOL = 0.4, 256.0
 METRIC = "GRays/s Ax + Gvox-upd/s Atb at 512^3"
 WORKLOAD = "cone-beam 512^3 @ 0.5 mm, 1024x768 det @ 0.4 mm, 720 views / 2pi, DSO 1000, DSD 1536"
 
 
+def set_size(size, views):
+    """--size 256: the 256^3 @ 1 mm / 512x512 @ 0.8 mm case used for profiling captures."""
+    global NV, NU, NA, NVOX, DDET, WORKLOAD
+    if size == 256:
+        NV, NU, NVOX, DDET = 512, 512, (256, 256, 256), 0.8
+        WORKLOAD = "cone-beam 256^3 @ 1 mm, 512x512 det @ 0.8 mm, %d views / 2pi, DSO 1000, DSD 1536"
+    if views:
+        NA = int(views)
+    if "%d" in WORKLOAD:
+        WORKLOAD = WORKLOAD % NA
+    elif views:
+        WORKLOAD = WORKLOAD.replace("720 views", "%d views" % NA)
+
+
 def geometry():
     from tigre_b200.utilities.geometry import cone_geometry
-    return cone_geometry(NVOX, (256.0, 256.0, 256.0), (NV, NU), (0.4, 0.4), DSO=1000.0, DSD=1536.0)
+    return cone_geometry(NVOX, (SVOL, SVOL, SVOL), (NV, NU), (DDET, DDET), DSO=1000.0, DSD=1536.0)
 
 
 def angles():
@@ -178,7 +193,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--size", type=int, default=512, choices=[512, 256])
+    ap.add_argument("--views", type=int, default=0)
     args = ap.parse_args()
+    set_size(args.size, args.views)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
