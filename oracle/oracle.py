@@ -157,3 +157,94 @@ def pocs_tv(img, alpha, maxiter, nthreads=0):
     lib().oracle_pocs_tv(img.ctypes.data, out.ctypes.data, float(alpha), nx, ny, nz, int(maxiter),
                          _threads(nthreads))
     return out
+
+
+# ---------------------------------------------------------------- FDK pieces --
+def fdk_filter(proj, geo, angles, filter=None):  # noqa: A002
+    """Cosine weighting + ramp filtering exactly as the reference's host path:
+    single_pass_algorithms.py:186-197 then filtering.py:15-53 (scipy.fft on
+    complex64, two projections per transform)."""
+    from scipy.fft import fft, ifft
+    g = copy.deepcopy(geo)
+    g.check_geo(angles)
+    nv, nu = int(g.nDetector[0]), int(g.nDetector[1])
+    du, dv = float(g.dDetector[1]), float(g.dDetector[0])
+    xv = np.arange(-nu / 2 + 0.5, 1 + nu / 2 - 0.5) * du
+    yv = np.arange(-nv / 2 + 0.5, 1 + nv / 2 - 0.5) * dv
+    yy, xx = np.meshgrid(xv, yv)
+    dsd, dso = float(g.DSD[0]), float(g.DSO[0])
+    w = dsd / np.sqrt(dsd ** 2 + xx ** 2 + yy ** 2)
+    p = np.multiply(np.asarray(proj, dtype=np.float32), w).astype(np.float32)
+
+    def nextpow2(n):
+        i = 1
+        while (2 ** i) <= n:
+            i += 1
+        return i
+
+    L = max(64, 2 ** nextpow2(2 * nu))
+    nn = np.arange(-L / 2, L / 2)
+    h = np.zeros(nn.shape, dtype=np.float32)
+    h[int(L / 2)] = 1 / 4
+    odd = nn % 2 == 1
+    h[odd] = -1 / (np.pi * nn[odd]) ** 2
+    fk = abs(np.fft.fft(h)) * 2
+    filt = fk[: int(L / 2 + 1)]
+    wv = 2 * np.pi * np.arange(len(filt)) / L
+    if filter == "shepp_logan":
+        filt[1:] *= np.sin(wv[1:] / 2) / (wv[1:] / 2)
+    elif filter == "cosine":
+        filt[1:] *= np.cos(wv[1:] / 2)
+    elif filter == "hamming":
+        filt[1:] *= 0.54 + 0.46 * np.cos(wv[1:])
+    elif filter == "hann":
+        filt[1:] *= (1 + np.cos(wv[1:])) / 2
+    filt[wv > np.pi] = 0
+    filt = np.hstack((filt, filt[1:-1][::-1])).astype(np.float32)
+    filt = np.kron(np.ones((nv, 1), dtype=np.float32), filt)
+    pad = int((L - nu) // 2)
+    n = p.shape[0]
+    scale = (dsd / dso) * (2 * np.pi / n) / (4 * du)
+    f = np.empty((nv, L), dtype=np.complex64)
+    for i in range(0, n - 1, 2):
+        f.fill(0)
+        f.real[:, pad:pad + nu] = p[i]
+        f.imag[:, pad:pad + nu] = p[i + 1]
+        f = ifft(fft(f, axis=1) * filt, axis=1)
+        p[i] = f.real[:, pad:pad + nu] * scale
+        p[i + 1] = f.imag[:, pad:pad + nu] * scale
+    if n % 2:
+        f.fill(0)
+        f.real[:, pad:pad + nu] = p[n - 1]
+        f = np.real(ifft(fft(f, axis=1) * filt, axis=1))
+        p[n - 1] = f[:, pad:pad + nu] * scale
+    return p
+
+
+def fdk(proj, geo, angles, filter=None):  # noqa: A002
+    return atb(fdk_filter(proj, geo, angles, filter), geo, angles, "FDK")
+
+
+def cgls(proj, geo, angles, niter):
+    """CGLS of krylov_subspace_algorithms.py:39-97 with FP64 vectors over the oracle pair."""
+    b = np.asarray(proj, dtype=np.float64)
+    x = np.zeros(tuple(int(v) for v in geo.nVoxel), dtype=np.float64)
+    r = b.copy()
+    p = atb(r.astype(np.float32), geo, angles, "matched").astype(np.float64)
+    gamma = float((p * p).sum())
+    res = []
+    for _ in range(niter):
+        q = ax(p.astype(np.float32), geo, angles, "Siddon").astype(np.float64)
+        alpha = gamma / float((q * q).sum())
+        x += alpha * p
+        r -= alpha * q
+        rn = float(np.sqrt((r * r).sum()))
+        if res and rn > res[-1]:
+            x -= alpha * p
+            break
+        res.append(rn)
+        s = atb(r.astype(np.float32), geo, angles, "matched").astype(np.float64)
+        g1 = float((s * s).sum())
+        p = s + (g1 / gamma) * p
+        gamma = g1
+    return x.astype(np.float32), np.asarray(res)

@@ -1,0 +1,8 @@
+"""Device-resident algorithm drivers with the reference's names and signatures
+(Python/tigre/algorithms/__init__.py): fdk/FDK, cgls, ossart, sirt, sart, asd_pocs."""
+from .krylov import cgls, cgls_device  # noqa: F401
+from .single_pass import FDK, fdk, fbp, fdk_device  # noqa: F401
+from .art import ossart, sirt, sart, ART  # noqa: F401
+from .pocs import asd_pocs  # noqa: F401
+
+__all__ = ["FDK", "fdk", "fbp", "cgls", "ossart", "sirt", "sart", "asd_pocs"]

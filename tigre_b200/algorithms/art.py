@@ -1,0 +1,148 @@
+"""SART family (OS-SART, SIRT, SART), device-resident.
+
+Same algorithm as the reference's IterativeReconAlg
+(Python/tigre/algorithms/iterative_recon_alg.py:131-401, art_family_algorithms.py):
+
+    W = 1 / A(ones) on a 2^3 box enlarged to the detector (set_w, :214-230)
+    V_j = mean_z A_j^T(ones) (FDK backprojector, shrunk box) per subset (set_v, :232-270)
+    per subset j:  x += lambda / V_j * A_j^T_FDK( W_j * (b_j - A_j x) );  x = max(x, 0)
+
+Per subset the forward projection, the weighted residual, the FDK
+backprojection and the update run on the GPU; subsets that are contiguous
+view ranges reuse the full plan (angle_range), others get their own plan.
+Storage precision (extension): storage=torch.bfloat16/float16 keeps the
+volume and the projections in that type (FP32 arithmetic, FP64 geometry).
+"""
+from __future__ import annotations
+
+import copy
+
+import numpy as np
+
+from .. import _native as N
+from .. import projectors as P
+from ..utilities.order_subsets import order_subsets
+from ._common import Problem, torch
+
+
+class ART:
+    def __init__(self, prob: Problem, blocksize, order=None, lmbda=1.0, noneg=True, storage=None, verbose=False):
+        T = torch()
+        self.prob = prob
+        self.lmbda = float(lmbda)
+        self.noneg = noneg
+        self.verbose = verbose
+        self.storage = storage or T.float32
+        g = prob.geo
+        self.blocks, self.index = order_subsets(prob.angles, blocksize, order)
+        self.index = [np.asarray(i).reshape(-1).astype(np.int64) for i in self.index]
+        self.W = self._weights_w()
+        self.V = self._weights_v()
+        self.plans = []
+        for idx in self.index:
+            rng = prob.contiguous_range(idx)
+            if rng is not None:
+                self.plans.append((prob.plan, rng))
+            else:
+                sub = prob.sub_geometry(idx)
+                self.plans.append((N.get_plan(N.checked_geometry(sub, sub.angles), prob.device.index), None))
+        self.b = prob.b.to(self.storage) if self.storage != T.float32 else prob.b
+
+    def _weights_w(self):
+        T = torch()
+        prob = self.prob
+        gx = copy.deepcopy(prob.geo)
+        gx.sVoxel = np.array(gx.sVoxel, dtype=np.float64)
+        gx.sVoxel[1:] = gx.sVoxel[1:] * 1.1
+        gx.sVoxel[0] = max(float(gx.sDetector[0]), gx.sVoxel[0])
+        gx.nVoxel = np.array([2, 2, 2])
+        gx.dVoxel = gx.sVoxel / gx.nVoxel
+        plan = N.get_plan(N.checked_geometry(gx, prob.angles), prob.device.index)
+        W = P.ax(T.ones((2, 2, 2), dtype=T.float32, device=prob.device), plan, "Siddon")
+        W[W <= float(min(np.asarray(prob.geo.dVoxel) / 2))] = float("inf")
+        return 1.0 / W
+
+    def _weights_v(self):
+        T = torch()
+        prob = self.prob
+        g = prob.geo
+        V = []
+        for idx in self.index:
+            gx = prob.sub_geometry(idx)
+            sv = np.array(gx.sVoxel, dtype=np.float64)
+            gx.sVoxel = sv * np.max(sv[1:] / np.linalg.norm(sv[1:])) * 0.9
+            gx.dVoxel = gx.sVoxel / gx.nVoxel
+            plan = N.get_plan(N.checked_geometry(gx, gx.angles), prob.device.index)
+            ones = T.ones((len(idx),) + tuple(int(v) for v in g.nDetector), dtype=T.float32, device=prob.device)
+            v = P.atb(ones, plan, "FDK").mean(dim=0)
+            v[v == 0.0] = float("inf")
+            V.append(v.contiguous())
+        return V
+
+    def sweep(self, x):
+        """One pass over all subsets (art_data_minimizing)."""
+        T = torch()
+        for j, idx in enumerate(self.index):
+            plan, rng = self.plans[j]
+            if rng is not None:
+                b_j = self.b[rng[0]:rng[1]]
+                w_j = self.W[rng[0]:rng[1]]
+                est = P.ax(x, plan, "Siddon", angle_range=rng, out_dtype=T.float32)
+            else:
+                ii = T.as_tensor(idx, device=x.device)
+                b_j = self.b.index_select(0, ii)
+                w_j = self.W.index_select(0, ii)
+                est = P.ax(x, plan, "Siddon", out_dtype=T.float32)
+            err = (w_j * (b_j.float() - est)).contiguous()
+            bp = P.atb(err, plan, "FDK", angle_range=rng, out_dtype=T.float32)
+            upd = x.float() + (self.lmbda / self.V[j]).unsqueeze(0) * bp
+            if self.noneg:
+                upd.clamp_(min=0)
+            x.copy_(upd)
+        return x
+
+
+def _run(proj, geo, angles, niter, blocksize, kwargs):
+    prob = Problem(proj, geo, angles, kwargs.get("gpuids"))
+    T = torch()
+    storage = kwargs.get("storage", None)
+    art = ART(prob, blocksize, kwargs.get("OrderStrategy"), kwargs.get("lmbda", 1.0), kwargs.get("noneg", True),
+              storage, kwargs.get("verbose", False))
+    init = kwargs.get("init", None)
+    if isinstance(init, str) and init == "FDK":
+        from .single_pass import fdk_device
+        x = fdk_device(prob).clamp_(min=0)
+    elif init is not None and not isinstance(init, str):
+        x = prob.to_device_vol(init)
+    else:
+        x = prob.zeros_vol()
+    if storage is not None and storage != T.float32:
+        x = x.to(storage)
+    l2 = []
+    callback = kwargs.get("callback")
+    for it in range(niter):
+        art.sweep(x)
+        if kwargs.get("computel2", False):
+            l2.append(float(T.linalg.vector_norm((prob.b - P.ax(x, prob.plan, "Siddon", out_dtype=T.float32))
+                                                 .double()).item()))
+        if callback is not None:
+            callback(it, x)
+    out = prob.out(x.float() if x.dtype != T.float32 else x)
+    if kwargs.get("computel2", False):
+        return out, np.asarray(l2, dtype=np.float32).reshape(1, -1)
+    return out
+
+
+def ossart(proj, geo, angles, niter, **kwargs):
+    """Drop-in for tigre.algorithms.ossart (blocksize default 20)."""
+    return _run(proj, geo, angles, niter, kwargs.pop("blocksize", 20), kwargs)
+
+
+def sirt(proj, geo, angles, niter, **kwargs):
+    kwargs.pop("blocksize", None)
+    return _run(proj, geo, angles, niter, len(np.atleast_1d(angles)), kwargs)
+
+
+def sart(proj, geo, angles, niter, **kwargs):
+    kwargs.pop("blocksize", None)
+    return _run(proj, geo, angles, niter, 1, kwargs)

@@ -60,6 +60,12 @@ int tigre_ax(TigrePlan* plan, const void* d_vol, int vdt, void* d_proj, int pdt,
     layouts_needed(plan, a0, a1, l0, l1);
     const size_t es = dtype_size(vdt);
     int rc = TIGRE_SUCCESS;
+    if (projector == TIGRE_PROJ_SIDDON && plan->columns) {
+        void* s = plan_scratch(plan, (size_t)d.nX * d.nY * (d.nZ + 2) * es, st, &rc);
+        if (rc) return rc;
+        if ((rc = launch_make_zfast(d_vol, vdt, s, d.nX, d.nY, d.nZ, st))) return rc;
+        return launch_siddon_columns(plan, s, vdt, d_proj, pdt, a0, a1, st);
+    }
     if (projector == TIGRE_PROJ_SIDDON) {
         const void* vx = d_vol;
         const void* vy = nullptr;

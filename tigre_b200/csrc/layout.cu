@@ -52,6 +52,26 @@ __global__ void make_layout_kernel(const T* __restrict__ src, T* __restrict__ ds
     }
 }
 
+// z-fastest copy: dst (X, Y, Z+2), dst[(x*Y + y)*(Z+2) + zp] = src(z = zp-1, y, x), zeros at zp = 0, Z+1.
+// One y per block row of the grid; a 32x32 (zp, x) tile goes through shared memory.
+template <typename T>
+__global__ void make_zfast_kernel(const T* __restrict__ src, T* __restrict__ dst, int nX, int nY, int nZ) {
+    __shared__ T tile[TILE][TILE + 1];
+    const int ZP = nZ + 2;
+    const int zp0 = blockIdx.x * TILE, x0 = blockIdx.y * TILE, y = blockIdx.z;
+    for (int j = threadIdx.y; j < TILE; j += blockDim.y) {
+        const int zp = zp0 + j, x = x0 + threadIdx.x, z = zp - 1;
+        T v = from_f32<T>(0.f);
+        if (z >= 0 && z < nZ && x < nX) v = src[((size_t)z * nY + y) * nX + x];
+        tile[j][threadIdx.x] = v;
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < TILE; j += blockDim.y) {
+        const int x = x0 + j, zp = zp0 + threadIdx.x;
+        if (x < nX && zp < ZP) dst[((size_t)x * nY + y) * ZP + zp] = tile[threadIdx.x][j];
+    }
+}
+
 template <typename T>
 __global__ void pad_projections_kernel(const T* __restrict__ src, T* __restrict__ dst, int nV, int nU, long total) {
     const long pitch = bp_pitch(nU), rows = bp_rows(nV);
@@ -79,6 +99,14 @@ int launch_make_layout(const void* src, int dtype, void* dst, int nX, int nY, in
         else
             make_layout_kernel<T, 1><<<grid, block, 0, st>>>((const T*)src, (T*)dst, nX, nY, nZ, pad_lo, pad_hi);
     });
+    TIGRE_CUDA(cudaGetLastError());
+    return TIGRE_SUCCESS;
+}
+
+int launch_make_zfast(const void* src, int dtype, void* dst, int nX, int nY, int nZ, cudaStream_t st) {
+    dim3 block(TILE, 8);
+    dim3 grid((nZ + 2 + TILE - 1) / TILE, (nX + TILE - 1) / TILE, nY);
+    TIGRE_DISPATCH_DTYPE(dtype, T, { make_zfast_kernel<T><<<grid, block, 0, st>>>((const T*)src, (T*)dst, nX, nY, nZ); });
     TIGRE_CUDA(cudaGetLastError());
     return TIGRE_SUCCESS;
 }

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <cstdlib>
 #include <mutex>
 
 #include "tigre_internal.h"
@@ -111,7 +112,7 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
     plan->h_siddon.resize(nangles);
     plan->h_interp.resize(nangles);
     plan->h_bp.resize(nangles);
-    bool axial = true;
+    bool axial = true, columns = true;
     for (int i = 0; i < nangles; ++i) {
         const double al = angles[3 * i], th = angles[3 * i + 1], ps = angles[3 * i + 2];
         const double dso = g->DSO[i], dsd = g->DSD[i];
@@ -144,6 +145,7 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
         // neighbouring detector columns move mostly along y -> y-fastest working copy
         fs.layout = std::fabs(Pu.y) >= std::fabs(Pu.x) ? 1 : 0;
         fs.pad_ = 0;
+        if (Pv.x != 0.0 || Pv.y != 0.0) columns = false;
 
         // ---- interpolated frame: voxel centres at integers (computeDeltas) ----
         FrameInterp& fi = plan->h_interp[i];
@@ -210,6 +212,7 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
         }
     }
     plan->axial = axial;
+    plan->columns = columns && std::getenv("TIGRE_B200_GENERIC_SIDDON") == nullptr;
     return TIGRE_SUCCESS;
 }
 

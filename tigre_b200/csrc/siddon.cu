@@ -196,6 +196,136 @@ __global__ void __launch_bounds__(256) siddon_count_kernel(SiddonArgs p) {
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(p.count, c);
 }
 
+// ---------------------------------------------------------------------------
+// Column-coherent Siddon.  When the detector's v axis is parallel to the
+// volume's z axis (no tilt: theta = psi = 0 and no detector roll/pitch/yaw),
+// every ray of one detector column lies in the same vertical plane through the
+// source: all of them share x- and y-components of direction and therefore
+// the same sequence of x/y plane crossings.  One warp takes one column and
+// 32*R of its rows (row = lane + 32 r): the xy traversal is warp-uniform (no
+// divergence), and each row only adds its own z crossings, which are rare at
+// cone-beam angles.  The volume is read from a z-fastest copy (x, y, z) with
+// one zero voxel before and after each z-run, so the 32 lanes of a warp load
+// ~17 consecutive floats of the same (x, y) column per step, and a ray that
+// leaves the volume through its top or bottom reads zeros.  Grid order
+// (column groups fastest, then views, then row tiles) keeps the z-slab of the
+// current row tile L2-resident while every view is processed.
+template <typename TV, typename TP, int R>
+__global__ void __launch_bounds__(128) siddon_columns_kernel(SiddonArgs p) {
+    const int lane = threadIdx.x & 31;
+    const int u = blockIdx.x * 4 + (threadIdx.x >> 5);
+    const int la = blockIdx.y;
+    if (u >= p.nU) return;
+    const FrameSiddon& F = p.frames[p.a0 + la];
+    const int vbase = blockIdx.z * (32 * R) + lane;
+    TP* out = (TP*)p.proj + (size_t)la * p.nV * p.nU + u;
+    // ---- shared xy ray (identical in every lane of the warp) ----
+    double rx = fma((double)u, F.du[0], F.o[0]) - F.s[0];
+    double ry = fma((double)u, F.du[1], F.o[1]) - F.s[1];
+    if (fabs(rx) < 0.001) rx = 0.0;   // Siddon_projection.cu:156-159
+    if (fabs(ry) < 0.001) ry = 0.0;
+    double am = -1e300, aM = 1e300;
+    bool miss = false;
+    if (rx != 0.0) {
+        const double i = 1.0 / rx, a0 = -F.s[0] * i, a1 = ((double)p.nX - F.s[0]) * i;
+        am = fmax(am, fmin(a0, a1)); aM = fmin(aM, fmax(a0, a1));
+    } else if (F.s[0] < 0.0 || F.s[0] > (double)p.nX) miss = true;
+    if (ry != 0.0) {
+        const double i = 1.0 / ry, a0 = -F.s[1] * i, a1 = ((double)p.nY - F.s[1]) * i;
+        am = fmax(am, fmin(a0, a1)); aM = fmin(aM, fmax(a0, a1));
+    } else if (F.s[1] < 0.0 || F.s[1] > (double)p.nY) miss = true;
+    if (miss || !(am < aM)) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int v = vbase + 32 * r;
+            if (v < p.nV) out[(size_t)v * p.nU] = from_f32<TP>(0.f);
+        }
+        return;
+    }
+    const AxisSetup ax = axis_setup(F.s[0], rx, am, aM, p.nX);
+    const AxisSetup ay = axis_setup(F.s[1], ry, am, aM, p.nY);
+    const int ncells = 1 + (int)ax.ncross + (int)ay.ncross;
+    const float T = (float)(aM - am);
+    // ---- per-row z state ----
+    int iz[R], sz[R];
+    float tz[R], tz0[R], dtz[R], kz[R], sum[R], len[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int v = min(vbase + 32 * r, p.nV - 1);
+        const double pv = (double)(p.nV - 1 - v);
+        double rz = fma(pv, F.dv[2], fma((double)u, F.du[2], F.o[2])) - F.s[2];
+        if (fabs(rz) < 0.001) rz = 0.0;
+        const double ze = fma(am, rz, F.s[2]);
+        int z = (int)fmin(fmax(floor(ze), -1.0), (double)p.nZ);
+        iz[r] = z;
+        sum[r] = 0.f;
+        kz[r] = 0.f;
+        len[r] = (float)sqrt(rx * rx * p.dVX * p.dVX + ry * ry * p.dVY * p.dVY + rz * rz * p.dVZ * p.dVZ);
+        if (rz > 0.0 && z < p.nZ) {
+            sz[r] = 1;
+            tz0[r] = (float)(((double)(z + 1) - F.s[2]) / rz - am);
+            dtz[r] = (float)(1.0 / rz);
+        } else if (rz < 0.0 && z >= 0) {
+            sz[r] = -1;
+            tz0[r] = (float)(((double)z - F.s[2]) / rz - am);
+            dtz[r] = (float)(-1.0 / rz);
+        } else {
+            sz[r] = 0;
+            tz0[r] = kInf;
+            dtz[r] = 0.f;
+        }
+        tz[r] = tz0[r];
+    }
+    const TV* __restrict__ vol = (const TV*)p.vol_x;
+    const int ZP = p.nZ + 2;
+    int cidx = ax.i * p.nY + ay.i;
+    const int dcx = ax.step * p.nY, dcy = ay.step;
+    int remx = ax.rem, remy = ay.rem;
+    float tx = ax.t0, ty = ay.t0, kx = 0.f, ky = 0.f;
+    float a = 0.f;
+#pragma unroll 1
+    for (int c = 0; c < ncells; ++c) {
+        const float tn = fminf(tx, ty);
+        const float b = fminf(tn, T);
+        const TV* col = vol + cidx * ZP + 1;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            float val = ldg_f<TV>(col + iz[r]);
+            if (tz[r] < b) {
+                // z crossings inside this cell (rare at cone-beam angles)
+                float st = a;
+                do {
+                    sum[r] = fmaf(tz[r] - st, val, sum[r]);
+                    st = tz[r];
+                    iz[r] += sz[r];
+                    kz[r] += 1.f;
+                    const bool more = sz[r] > 0 ? iz[r] < p.nZ : iz[r] >= 0;
+                    tz[r] = more ? fmaf(kz[r], dtz[r], tz0[r]) : kInf;
+                    val = ldg_f<TV>(col + iz[r]);
+                } while (tz[r] < b);
+                sum[r] = fmaf(b - st, val, sum[r]);
+            } else {
+                sum[r] = fmaf(b - a, val, sum[r]);
+            }
+        }
+        a = b;
+        if (tx <= ty) {
+            cidx += dcx;
+            kx += 1.f;
+            tx = (--remx > 0) ? fmaf(kx, ax.dt, ax.t0) : kInf;
+        } else {
+            cidx += dcy;
+            ky += 1.f;
+            ty = (--remy > 0) ? fmaf(ky, ay.dt, ay.t0) : kInf;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int v = vbase + 32 * r;
+        if (v < p.nV) out[(size_t)v * p.nU] = from_f32<TP>(sum[r] * len[r]);
+    }
+}
+
 SiddonArgs make_args(TigrePlan* P, int a0) {
     SiddonArgs a{};
     a.frames = P->d_siddon;
@@ -233,6 +363,39 @@ int launch_siddon(TigrePlan* P, const void* vol_x, const void* vol_y, int vdt, v
         else if (vdt == TIGRE_F32 && pdt == TIGRE_BF16)
             siddon_kernel<float, __nv_bfloat16><<<grid, block, 0, st>>>(ac);
         else if (vdt == TIGRE_F32 && pdt == TIGRE_F16) siddon_kernel<float, __half><<<grid, block, 0, st>>>(ac);
+        else return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype pair for Siddon");
+        TIGRE_CUDA(cudaGetLastError());
+    }
+    return TIGRE_SUCCESS;
+}
+
+template <typename TV, typename TP>
+static void launch_columns_typed(const SiddonArgs& a, int rows_per_thread, dim3 grid, cudaStream_t st) {
+    if (rows_per_thread == 4) siddon_columns_kernel<TV, TP, 4><<<grid, 128, 0, st>>>(a);
+    else if (rows_per_thread == 2) siddon_columns_kernel<TV, TP, 2><<<grid, 128, 0, st>>>(a);
+    else siddon_columns_kernel<TV, TP, 1><<<grid, 128, 0, st>>>(a);
+}
+
+int launch_siddon_columns(TigrePlan* P, const void* vol_z, int vdt, void* proj, int pdt, int a0, int a1,
+                          cudaStream_t st) {
+    SiddonArgs a = make_args(P, a0);
+    a.vol_x = vol_z;
+    a.proj = proj;
+    const int nv = P->d.nV;
+    const int R = nv >= 512 ? 4 : (nv >= 128 ? 2 : 1);
+    const int na = a1 - a0;
+    for (int c = 0; c < na; c += 65535) {
+        SiddonArgs ac = a;
+        ac.a0 = a0 + c;
+        ac.proj = (char*)proj + (size_t)c * P->d.nU * P->d.nV * dtype_size(pdt);
+        dim3 grid((P->d.nU + 3) / 4, std::min(65535, na - c), (nv + 32 * R - 1) / (32 * R));
+        if (vdt == TIGRE_F32 && pdt == TIGRE_F32) launch_columns_typed<float, float>(ac, R, grid, st);
+        else if (vdt == TIGRE_BF16 && pdt == TIGRE_BF16) launch_columns_typed<__nv_bfloat16, __nv_bfloat16>(ac, R, grid, st);
+        else if (vdt == TIGRE_F16 && pdt == TIGRE_F16) launch_columns_typed<__half, __half>(ac, R, grid, st);
+        else if (vdt == TIGRE_BF16 && pdt == TIGRE_F32) launch_columns_typed<__nv_bfloat16, float>(ac, R, grid, st);
+        else if (vdt == TIGRE_F16 && pdt == TIGRE_F32) launch_columns_typed<__half, float>(ac, R, grid, st);
+        else if (vdt == TIGRE_F32 && pdt == TIGRE_BF16) launch_columns_typed<float, __nv_bfloat16>(ac, R, grid, st);
+        else if (vdt == TIGRE_F32 && pdt == TIGRE_F16) launch_columns_typed<float, __half>(ac, R, grid, st);
         else return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype pair for Siddon");
         TIGRE_CUDA(cudaGetLastError());
     }

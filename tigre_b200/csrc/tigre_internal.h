@@ -88,6 +88,7 @@ struct TigrePlan {
     tigre::FrameInterp* d_interp = nullptr;
     tigre::FrameBP* d_bp = nullptr;
     bool axial = false;          // every BP frame has dz.x == dz.y == 0 (u constant along z)
+    bool columns = false;        // every Siddon frame has dv.x == dv.y == 0 (detector v parallel to z)
     // growable stream-ordered scratch arena
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -102,10 +103,13 @@ void* plan_scratch(TigrePlan* plan, size_t bytes, cudaStream_t st, int* rc);
 int launch_make_layout(const void* src, int dtype, void* dst, int nX, int nY, int nZ, int layout, int pad_lo,
                        int pad_hi, cudaStream_t st);
 int launch_pad_projections(const void* src, int dtype, void* dst, int nA, int nV, int nU, cudaStream_t st);
+int launch_make_zfast(const void* src, int dtype, void* dst, int nX, int nY, int nZ, cudaStream_t st);
 
 int launch_siddon(TigrePlan* p, const void* vol_x, const void* vol_y, int vdt, void* proj, int pdt, int a0, int a1,
                   cudaStream_t st);
 int launch_siddon_count(TigrePlan* p, int a0, int a1, unsigned long long* d_total, cudaStream_t st);
+int launch_siddon_columns(TigrePlan* p, const void* vol_z, int vdt, void* proj, int pdt, int a0, int a1,
+                          cudaStream_t st);
 int launch_interp(TigrePlan* p, const void* vol_x, const void* vol_y, int vdt, void* proj, int pdt, int a0, int a1,
                   cudaStream_t st);
 int launch_backproject(TigrePlan* p, const void* proj_pad, int pdt, void* vol, int vdt, int matched, int a0, int a1,

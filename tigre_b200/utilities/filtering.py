@@ -66,15 +66,18 @@ def ramp_response(nU, filter=None):  # noqa: A002,N803
     return L, filter_kernel(filter, ramp_flat(L)[0], L)
 
 
-def filter_projections(proj, geo, nangles, filter=None, precision="float32"):  # noqa: A002
-    """Ramp-filter device projections (n, nV, nU) in place-free fashion; returns a new tensor."""
+def filter_projections(proj, geo, nangles, filter=None, precision="float32", angular_weight=None):  # noqa: A002
+    """Ramp-filter device projections (n, nV, nU); returns a new tensor.  angular_weight
+    replaces 2 pi / nangles (short scans with Parker weights use 2 * mean view step,
+    MATLAB/Utilities/filtering.m:47-48)."""
     import torch
     nU = proj.shape[-1]
     L, filt = ramp_response(nU, filter)
     pad = int((L - nU) // 2)
     dsd = float(np.asarray(geo.DSD).reshape(-1)[0])
     dso = float(np.asarray(geo.DSO).reshape(-1)[0])
-    scale = (dsd / dso) * (2 * np.pi / nangles) / (4 * float(geo.dDetector[1]))
+    aw = (2 * np.pi / nangles) if angular_weight is None else float(angular_weight)
+    scale = (dsd / dso) * aw / (4 * float(geo.dDetector[1]))
     cdt = torch.float64 if precision == "float64" else torch.float32
     H = torch.from_numpy(filt[: L // 2 + 1].astype(np.float64)).to(device=proj.device, dtype=cdt)
     buf = torch.zeros(proj.shape[:-1] + (L,), dtype=cdt, device=proj.device)
@@ -148,8 +151,12 @@ def filtering(proj, geo, angles, parker, verbose=False):
     t = torch.from_numpy(np.ascontiguousarray(proj, dtype=np.float32))
     if torch.cuda.is_available():
         t = t.cuda()
+    aw = None
     if parker:
         W = torch.from_numpy(parker_weights(geo, angles, parker)).to(t.device)
         t = t * W[:, None, :]
-    out = filter_projections(t, geo, len(angles), getattr(geo, "filter", None))
+        a = np.asarray(angles, dtype=np.float64)
+        a = a[:, 0] if a.ndim == 2 else a
+        aw = 2 * np.mean(np.abs(np.diff(a)))
+    out = filter_projections(t, geo, len(angles), getattr(geo, "filter", None), angular_weight=aw)
     return out.cpu().numpy()
