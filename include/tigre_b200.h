@@ -139,6 +139,10 @@ int tigre_plan_create(const TigreGeometry* geo, const float* angles, int nangles
 void tigre_plan_destroy(TigrePlan* plan);
 /* Bytes of device scratch currently held by the plan. */
 long long tigre_plan_scratch_bytes(const TigrePlan* plan);
+/* Synchronises the plan's device and returns its kernel status word (0 = ok; bit 0:
+ * a bounded wait inside a kernel expired, results of that call are invalid).
+ * reset != 0 clears it. */
+int tigre_plan_status(TigrePlan* plan, int reset);
 
 /* Forward projection of d_vol (nZ,nY,nX) into d_proj ((angle_end-angle_begin), nV, nU)
  * for plan angles [angle_begin, angle_end).  projector: TIGRE_PROJ_*. */

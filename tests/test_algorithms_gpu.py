@@ -115,7 +115,8 @@ def test_autograd_loss_finite_differences():
     rng = np.random.default_rng(0)
     A = AG.A(geo, ang)
     b = torch.from_numpy(O.ax(img, geo, ang, "Siddon")).cuda().double()
-    x0 = torch.from_numpy((img + rng.normal(0, 2e-3, img.shape)).astype(np.float32)).cuda()
+    # noise >> h keeps every |grad f| term of the TV away from its kink during the differences
+    x0 = torch.from_numpy((img + rng.normal(0, 5e-2, img.shape)).astype(np.float32)).cuda()
 
     def loss(x):
         r = A(x).double() - b

@@ -73,6 +73,7 @@ _SIGS = {
     "tigre_plan_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "tigre_plan_destroy": (None, [C.c_void_p]),
     "tigre_plan_scratch_bytes": (C.c_longlong, [C.c_void_p]),
+    "tigre_plan_status": (C.c_int, [C.c_void_p, C.c_int]),
     "tigre_ax": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                            C.c_void_p]),
     "tigre_atb": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -205,6 +206,10 @@ class Plan:
 
     def scratch_bytes(self):
         return int(lib().tigre_plan_scratch_bytes(self.handle))
+
+    def status(self, reset=True):
+        """Kernel status word (0 = ok); synchronises the device."""
+        return int(lib().tigre_plan_status(self.handle, 1 if reset else 0))
 
 
 _plan_cache: "dict[str, Plan]" = {}

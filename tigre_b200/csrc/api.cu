@@ -10,6 +10,7 @@
 // errors come back as return codes instead of exit(1).
 
 #include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -102,6 +103,18 @@ int tigre_atb(TigrePlan* plan, const void* d_proj, int pdt, void* d_vol, int vdt
     const Dims& d = plan->d;
     const int na = a1 - a0;
     int rc = TIGRE_SUCCESS;
+    if (bp_tma_supported(plan, pdt)) {
+        const int align = 16 / (int)dtype_size(pdt);
+        if (d.nU % align == 0 && ((uintptr_t)d_proj % 16) == 0)
+            return launch_backproject_tma(plan, d_proj, d.nU, pdt, d_vol, vdt,
+                                          backprojector == TIGRE_BACKPROJ_MATCHED, a0, a1, st);
+        const int pitch = (d.nU + align - 1) / align * align;
+        void* s = plan_scratch(plan, (size_t)na * d.nV * pitch * dtype_size(pdt), st, &rc);
+        if (rc) return rc;
+        if ((rc = launch_repitch_projections(d_proj, pdt, s, na, d.nV, d.nU, pitch, st))) return rc;
+        return launch_backproject_tma(plan, s, pitch, pdt, d_vol, vdt, backprojector == TIGRE_BACKPROJ_MATCHED, a0,
+                                      a1, st);
+    }
     void* s = plan_scratch(plan, (size_t)na * bp_rows(d.nV) * bp_pitch(d.nU) * dtype_size(pdt), st, &rc);
     if (rc) return rc;
     if ((rc = launch_pad_projections(d_proj, pdt, s, na, d.nV, d.nU, st))) return rc;
@@ -227,6 +240,7 @@ int host_backproject(const float* proj, const TigreGeometry* geo, float* result,
         return rc;
     TIGRE_CUDA(cudaMemcpyAsync(result, dvol, nvox * sizeof(float), cudaMemcpyDeviceToHost, h.st));
     TIGRE_CUDA(cudaStreamSynchronize(h.st));
+    if (tigre_plan_status(h.plan, 1) != 0) return fail(TIGRE_ERR_CUDA, "backprojection: a bounded wait expired");
     return TIGRE_SUCCESS;
 }
 

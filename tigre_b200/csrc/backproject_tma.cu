@@ -1,0 +1,376 @@
+// Voxel-driven backprojection with TMA-staged projection patches (sm_100a).
+//
+// Same arithmetic as backproject.cu (FDK weight of voxel_backprojection.cu:242-249,
+// matched weight of voxel_backprojection2.cu:256-280, bilinear sampling with border 0),
+// organised for the B200 memory system:
+//
+//  * a block owns 16 x 16 voxel columns x 16 slices (one thread per column,
+//    16 accumulators in registers) and loops over every view of the call;
+//  * for each view, the bilinear footprint of the block's voxels lies inside
+//    the bounding box of its 8 projected corners; one elected lane issues a
+//    cp.async.bulk.tensor load of that box of the projection into shared
+//    memory (TMA zero-fills what lies outside the detector, which is exactly
+//    the texture border rule), double-buffered on two mbarriers so the next
+//    view's patch streams in while the current one is consumed;
+//  * all per-view constants are precomputed on the host (FrameBPK), so a
+//    (column, view) costs a few FP64 FMAs and one division, and a voxel
+//    update a handful of FP32 instructions and four shared-memory loads;
+//  * every mbarrier wait is bounded; on expiry the kernel records an error
+//    code in the plan's status word instead of hanging.
+// A (block, view) whose footprint does not fit the box (possible for strongly
+// magnified geometries) falls back to bounds-checked global loads.
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cmath>
+#include <mutex>
+
+#include "tigre_internal.h"
+
+namespace tigre {
+namespace {
+
+constexpr int TXY = 16;   // columns per block edge
+constexpr int VZ = 16;    // slices per thread
+constexpr unsigned kWaitLimit = 1u << 16;   // ~ a few ms with the back-off below
+
+struct BPKArgs {
+    const FrameBPK* frames;
+    const void* proj;     // projection buffer the tensor map describes (fallback reads)
+    void* vol;
+    int* status;
+    int a0, na;
+    int nX, nY, nZ, nU, nV;
+    int pitch;            // row pitch of proj in elements
+    int BU, BV;           // patch box
+    float dVZ;
+    float scale;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    for (unsigned i = 0; i < kWaitLimit; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        if (ok) return true;
+        __nanosleep(32);
+    }
+    return false;
+}
+
+// texel-space (u - 0.5, v - 0.5) projection of voxel (x, y, z) for view frame F
+__device__ __forceinline__ void project_texel(const FrameBPK& F, float x, float y, float z, float& ub, float& vb) {
+    const double vx = fma((double)z, F.dz[0], fma((double)y, F.dy[0], fma((double)x, F.dx[0], F.b[0])));
+    const double vy = fma((double)z, F.dz[1], fma((double)y, F.dy[1], fma((double)x, F.dx[1], F.b[1])));
+    const double vz = fma((double)z, F.dz[2], fma((double)y, F.dy[2], fma((double)x, F.dx[2], F.b[2])));
+    const float t = F.tnum / (float)vx;
+    ub = fmaf((float)vy, t, F.cu) - 0.5f;
+    vb = fmaf((float)vz, t, F.cv) - 0.5f;
+}
+
+// Warp 0: bounding box of the block's 8 corner voxels for local view la; lane 0 writes
+// info[] and issues the TMA load (or a plain arrive when the box does not fit).
+template <typename TP>
+__device__ __forceinline__ void plan_patch(const BPKArgs& p, const CUtensorMap* tmap, int la, int x0, int y0, int z0,
+                                           TP* dst, uint32_t bar, int* info) {
+    const int lane = threadIdx.x & 31;
+    const FrameBPK& F = p.frames[p.a0 + la];
+    float ub = 0.f, vb = 0.f;
+    if (lane < 8) {
+        const int x = min(x0 + ((lane & 1) ? TXY - 1 : 0), p.nX - 1);
+        const int y = min(y0 + ((lane & 2) ? TXY - 1 : 0), p.nY - 1);
+        const int z = min(z0 + ((lane & 4) ? VZ - 1 : 0), p.nZ - 1);
+        project_texel(F, (float)x, (float)y, (float)z, ub, vb);
+    }
+    float umin = lane < 8 ? ub : 3e38f, umax = lane < 8 ? ub : -3e38f;
+    float vmin = lane < 8 ? vb : 3e38f, vmax = lane < 8 ? vb : -3e38f;
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+        umin = fminf(umin, __shfl_xor_sync(0xffffffffu, umin, o));
+        umax = fmaxf(umax, __shfl_xor_sync(0xffffffffu, umax, o));
+        vmin = fminf(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+        vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+    }
+    if (lane == 0) {
+        constexpr int ALIGN = 16 / (int)sizeof(TP);   // TMA: x * sizeof(T) multiple of 16 bytes
+        bool fits = isfinite(umin) && isfinite(umax) && isfinite(vmin) && isfinite(vmax) &&
+                    fabsf(umin) < 1e7f && fabsf(vmin) < 1e7f;
+        int u0 = 0, v0 = 0;
+        if (fits) {
+            u0 = (int)floorf(umin) - 1;
+            u0 = (u0 >= 0) ? (u0 / ALIGN) * ALIGN : -(((-u0) + ALIGN - 1) / ALIGN) * ALIGN;
+            v0 = (int)floorf(vmin) - 1;
+            fits = ((int)ceilf(umax) + 2 - u0 <= p.BU - 1) && ((int)ceilf(vmax) + 2 - v0 <= p.BV - 1);
+        }
+        info[0] = u0;
+        info[1] = v0;
+        info[2] = fits ? 1 : 0;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        if (fits) {
+            const uint32_t bytes = (uint32_t)(p.BU * p.BV * sizeof(TP));
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+                "[%5];" ::"r"(smem_u32(dst)),
+                "l"((unsigned long long)tmap), "r"(u0), "r"(v0), "r"(la), "r"(bar)
+                : "memory");
+        } else {
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+        }
+    }
+}
+
+template <typename TP>
+__device__ __forceinline__ float patch_sample(const TP* patch, int BU, int iu, float fu, float pv, float pvmax) {
+    pv = fminf(fmaxf(pv, 0.f), pvmax);
+    const int iv = (int)pv;
+    const float fv = pv - (float)iv;
+    const TP* r0 = patch + iv * BU + iu;
+    const float p00 = to_f32<TP>(r0[0]), p01 = to_f32<TP>(r0[1]);
+    const float p10 = to_f32<TP>(r0[BU]), p11 = to_f32<TP>(r0[BU + 1]);
+    const float a0 = fmaf(fu, p01 - p00, p00), a1 = fmaf(fu, p11 - p10, p10);
+    return fmaf(fv, a1 - a0, a0);
+}
+
+template <typename TP>
+__device__ __forceinline__ float global_sample(const BPKArgs& p, const TP* P, float ub, float vb) {
+    const float fx = floorf(ub), fy = floorf(vb);
+    const float au = ub - fx, av = vb - fy;
+    const int iu = (int)fmaxf(fminf(fx, 1e8f), -1e8f), iv = (int)fmaxf(fminf(fy, 1e8f), -1e8f);
+    auto at = [&](int u, int v) -> float {
+        return (u >= 0 && u < p.nU && v >= 0 && v < p.nV) ? to_f32<TP>(P[(long)v * p.pitch + u]) : 0.f;
+    };
+    const float a0 = fmaf(au, at(iu + 1, iv) - at(iu, iv), at(iu, iv));
+    const float a1 = fmaf(au, at(iu + 1, iv + 1) - at(iu, iv + 1), at(iu, iv + 1));
+    return fmaf(av, a1 - a0, a0);
+}
+
+template <typename TP, typename TV, bool MATCHED, bool AXIAL>
+__global__ void __launch_bounds__(TXY* TXY) bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, BPKArgs p) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) unsigned long long bars[2];
+    __shared__ int info[2][4];
+    // TMA destinations: 128-byte aligned, each buffer rounded up to 128 bytes
+    const uint32_t base_off = (128u - (smem_u32(smem_raw) & 127u)) & 127u;
+    const size_t buf_bytes = ((size_t)p.BU * p.BV * sizeof(TP) + 127) / 128 * 128;
+    TP* buf0 = reinterpret_cast<TP*>(smem_raw + base_off);
+    TP* buf1 = reinterpret_cast<TP*>(smem_raw + base_off + buf_bytes);
+    const int tid = threadIdx.x;
+    const int tx = tid & (TXY - 1), ty = tid / TXY;
+    const int x0 = blockIdx.x * TXY, y0 = blockIdx.y * TXY, z0 = blockIdx.z * VZ;
+    const int x = x0 + tx, y = y0 + ty;
+    const bool active = x < p.nX && y < p.nY;
+    const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid < 32) {
+        plan_patch<TP>(p, &tmap, 0, x0, y0, z0, buf0, bar0, info[0]);
+        if (p.na > 1) plan_patch<TP>(p, &tmap, 1, x0, y0, z0, buf1, bar1, info[1]);
+    }
+    float acc[VZ];
+#pragma unroll
+    for (int k = 0; k < VZ; ++k) acc[k] = 0.f;
+    const TP* Pg = (const TP*)p.proj;
+    const float pumax = (float)(p.BU - 2), pvmax = (float)(p.BV - 2);
+    bool failed = false;
+    for (int la = 0; la < p.na; ++la) {
+        const int s = la & 1;
+        const uint32_t bar = s ? bar1 : bar0;
+        // after one expired wait the block stops waiting (its result is flagged invalid)
+        if (!failed && !mbar_wait(bar, (uint32_t)((la >> 1) & 1))) failed = true;
+        const TP* patch = s ? buf1 : buf0;
+        const int u0 = info[s][0], v0 = info[s][1], fits = info[s][2];
+        if (active) {
+            const FrameBPK& F = p.frames[p.a0 + la];
+            const double bxd = fma((double)z0, F.dz[0], fma((double)y, F.dy[0], fma((double)x, F.dx[0], F.b[0])));
+            const double byd = fma((double)z0, F.dz[1], fma((double)y, F.dy[1], fma((double)x, F.dx[1], F.b[1])));
+            const double bzd = fma((double)z0, F.dz[2], fma((double)y, F.dy[2], fma((double)x, F.dx[2], F.b[2])));
+            const float vx = (float)bxd, vy = (float)byd, vz = (float)bzd;
+            float wcol = 1.f, cu2 = 0.f, cxy = 0.f;
+            if (!MATCHED) {
+                const float den = fmaf((float)y, F.wy, fmaf((float)x, F.wx, F.w0));
+                const float r = F.dso / den;
+                wcol = r * r;
+            } else {
+                const float rvx = fmaf((float)x, F.dvx, F.rv0x), rvy = fmaf((float)y, F.dvy, F.rv0y);
+                cxy = (F.rsx - rvx) * (F.rsx - rvx) + (F.rsy - rvy) * (F.rsy - rvy);
+            }
+            if (AXIAL) {
+                const float t = F.tnum / vx;
+                const float u = fmaf(vy, t, F.cu);            // texture coordinate
+                const float vt0 = fmaf(vz, t, F.cv);
+                const float vstep = (float)F.dz[2] * t;
+                if (MATCHED) {
+                    const float day = fmaf(u, F.ddu, F.du0);
+                    const float dx = fmaf(day, F.sina, F.daxc), dy = fmaf(day, F.cosa, -F.daxs);
+                    cu2 = (F.rsx - dx) * (F.rsx - dx) + (F.rsy - dy) * (F.rsy - dy);
+                }
+                if (fits) {
+                    const float pu = fminf(fmaxf(u - 0.5f - (float)u0, 0.f), pumax);
+                    const int iu = (int)pu;
+                    const float fu = pu - (float)iu;
+                    const float pv0 = vt0 - 0.5f - (float)v0;
+#pragma unroll
+                    for (int k = 0; k < VZ; ++k) {
+                        const float smp = patch_sample<TP>(patch, p.BU, iu, fu, fmaf((float)k, vstep, pv0), pvmax);
+                        if (!MATCHED) {
+                            acc[k] = fmaf(smp, wcol, acc[k]);
+                        } else {
+                            const float vtex = fmaf((float)k, vstep, vt0);
+                            const float dz = fmaf(vtex, F.ddv, F.dzc);
+                            const float L2 = fmaf(dz, dz, cu2);
+                            const float rvz = fmaf((float)(z0 + k), p.dVZ, F.rv0z);
+                            const float lsq = fmaf(rvz, rvz, cxy);
+                            const float w = L2 * (L2 * rsqrtf(L2)) * __frcp_rn(F.dsd * lsq);
+                            acc[k] = fmaf(smp, w, acc[k]);
+                        }
+                    }
+                } else {
+#pragma unroll 1
+                    for (int k = 0; k < VZ; ++k) {
+                        const float vtex = fmaf((float)k, vstep, vt0);
+                        const float smp = global_sample<TP>(p, Pg + (long)la * p.pitch * p.nV, u - 0.5f, vtex - 0.5f);
+                        float w = wcol;
+                        if (MATCHED) {
+                            const float dz = fmaf(vtex, F.ddv, F.dzc);
+                            const float L2 = fmaf(dz, dz, cu2);
+                            const float rvz = fmaf((float)(z0 + k), p.dVZ, F.rv0z);
+                            const float lsq = fmaf(rvz, rvz, cxy);
+                            w = L2 * (L2 * rsqrtf(L2)) * __frcp_rn(F.dsd * lsq);
+                        }
+                        acc[k] = fmaf(smp, w, acc[k]);
+                    }
+                }
+            } else {
+                const float dzx = (float)F.dz[0], dzy = (float)F.dz[1], dzz = (float)F.dz[2];
+#pragma unroll
+                for (int k = 0; k < VZ; ++k) {
+                    const float kf = (float)k;
+                    const float ex = fmaf(kf, dzx, vx), ey = fmaf(kf, dzy, vy), ez = fmaf(kf, dzz, vz);
+                    const float t = F.tnum / ex;
+                    const float u = fmaf(ey, t, F.cu), vtex = fmaf(ez, t, F.cv);
+                    float smp;
+                    if (fits) {
+                        const float pu = fminf(fmaxf(u - 0.5f - (float)u0, 0.f), pumax);
+                        const int iu = (int)pu;
+                        smp = patch_sample<TP>(patch, p.BU, iu, pu - (float)iu, vtex - 0.5f - (float)v0, pvmax);
+                    } else {
+                        smp = global_sample<TP>(p, Pg + (long)la * p.pitch * p.nV, u - 0.5f, vtex - 0.5f);
+                    }
+                    float w = wcol;
+                    if (MATCHED) {
+                        const float day = fmaf(u, F.ddu, F.du0);
+                        const float dx = fmaf(day, F.sina, F.daxc), dy = fmaf(day, F.cosa, -F.daxs);
+                        const float dz = fmaf(vtex, F.ddv, F.dzc);
+                        const float L2 = (F.rsx - dx) * (F.rsx - dx) + (F.rsy - dy) * (F.rsy - dy) + dz * dz;
+                        const float rvz = fmaf((float)(z0 + k), p.dVZ, F.rv0z);
+                        const float lsq = fmaf(rvz, rvz, cxy);
+                        w = L2 * (L2 * rsqrtf(L2)) * __frcp_rn(F.dsd * lsq);
+                    }
+                    acc[k] = fmaf(smp, w, acc[k]);
+                }
+            }
+        }
+        __syncthreads();   // everyone is done with buffer s
+        if (tid < 32 && la + 2 < p.na) plan_patch<TP>(p, &tmap, la + 2, x0, y0, z0, s ? buf1 : buf0, bar, info[s]);
+    }
+    if (failed) {
+        // a copy may still be in flight: wait for the last phase of both buffers (bounded) before exiting
+        if (p.na > 0) mbar_wait(bar0, (uint32_t)(((p.na - 1 - ((p.na - 1) & 1)) >> 1) & 1));
+        if (p.na > 1) mbar_wait(bar1, (uint32_t)(((p.na - 1 - ((p.na - 1 + 1) & 1)) >> 1) & 1));
+        if (p.status) atomicOr(p.status, 1);
+    }
+    if (!active) return;
+    TV* V = (TV*)p.vol;
+#pragma unroll
+    for (int k = 0; k < VZ; ++k) {
+        const int z = z0 + k;
+        if (z < p.nZ) V[((size_t)z * p.nY + y) * p.nX + x] = from_f32<TV>(acc[k] * p.scale);
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    });
+    return fn;
+}
+
+template <typename TP, typename TV>
+int launch_typed(const CUtensorMap& tm, const BPKArgs& a, bool matched, bool axial, cudaStream_t st) {
+    dim3 grid((a.nX + TXY - 1) / TXY, (a.nY + TXY - 1) / TXY, (a.nZ + VZ - 1) / VZ);
+    const size_t smem = 2 * (((size_t)a.BU * a.BV * sizeof(TP) + 127) / 128 * 128) + 128;
+    auto go = [&](auto kern) -> int {
+        TIGRE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<grid, TXY * TXY, smem, st>>>(tm, a);
+        TIGRE_CUDA(cudaGetLastError());
+        return TIGRE_SUCCESS;
+    };
+    if (matched) return axial ? go(bp_tma_kernel<TP, TV, true, true>) : go(bp_tma_kernel<TP, TV, true, false>);
+    return axial ? go(bp_tma_kernel<TP, TV, false, true>) : go(bp_tma_kernel<TP, TV, false, false>);
+}
+
+}  // namespace
+
+bool bp_tma_supported(const TigrePlan* P, int pdt) {
+    if (pdt == TIGRE_F16) return false;
+    return P->bp_box_u > 0 && encode_fn() != nullptr;
+}
+
+int launch_backproject_tma(TigrePlan* P, const void* proj, int pitch, int pdt, void* vol, int vdt, int matched,
+                           int a0, int a1, cudaStream_t st) {
+    auto enc = encode_fn();
+    if (!enc) return fail(TIGRE_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    const int na = a1 - a0;
+    const size_t es = dtype_size(pdt);
+    CUtensorMap tm;
+    cuuint64_t dims[3] = {(cuuint64_t)pitch, (cuuint64_t)P->d.nV, (cuuint64_t)na};
+    cuuint64_t strides[2] = {(cuuint64_t)pitch * es, (cuuint64_t)pitch * P->d.nV * es};
+    cuuint32_t box[3] = {(cuuint32_t)P->bp_box_u, (cuuint32_t)P->bp_box_v, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(&tm, pdt == TIGRE_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3,
+                     const_cast<void*>(proj), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(TIGRE_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    BPKArgs a{};
+    a.frames = P->d_bpk;
+    a.proj = proj;
+    a.vol = vol;
+    a.status = P->d_status;
+    a.a0 = a0;
+    a.na = na;
+    a.nX = P->d.nX; a.nY = P->d.nY; a.nZ = P->d.nZ; a.nU = P->d.nU; a.nV = P->d.nV;
+    a.pitch = pitch;
+    a.BU = P->bp_box_u;
+    a.BV = P->bp_box_v;
+    a.dVZ = (float)P->d.dVZ;
+    a.scale = matched ? (float)(P->d.dVX * P->d.dVY * P->d.dVZ / (P->d.dDU * P->d.dDV)) : 1.f;
+    const bool ax = P->axial;
+    if (pdt == TIGRE_F32 && vdt == TIGRE_F32) return launch_typed<float, float>(tm, a, matched, ax, st);
+    if (pdt == TIGRE_BF16 && vdt == TIGRE_BF16) return launch_typed<__nv_bfloat16, __nv_bfloat16>(tm, a, matched, ax, st);
+    if (pdt == TIGRE_BF16 && vdt == TIGRE_F32) return launch_typed<__nv_bfloat16, float>(tm, a, matched, ax, st);
+    if (pdt == TIGRE_F32 && vdt == TIGRE_BF16) return launch_typed<float, __nv_bfloat16>(tm, a, matched, ax, st);
+    return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype pair for the staged backprojector");
+}
+
+}  // namespace tigre

@@ -86,7 +86,27 @@ __global__ void pad_projections_kernel(const T* __restrict__ src, T* __restrict_
     }
 }
 
+template <typename T>
+__global__ void repitch_kernel(const T* __restrict__ src, T* __restrict__ dst, int nU, int pitch, long rows) {
+    const long total = rows * pitch;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const long r = i / pitch;
+        const int c = (int)(i - r * pitch);
+        dst[i] = c < nU ? src[r * nU + c] : from_f32<T>(0.f);
+    }
+}
+
 }  // namespace
+
+int launch_repitch_projections(const void* src, int dtype, void* dst, int nA, int nV, int nU, int pitch,
+                               cudaStream_t st) {
+    const long rows = (long)nA * nV;
+    const long want = (rows * pitch + 255) / 256;
+    const int grid = (int)std::min<long>(want, 148L * 32);
+    TIGRE_DISPATCH_DTYPE(dtype, T, { repitch_kernel<T><<<grid, 256, 0, st>>>((const T*)src, (T*)dst, nU, pitch, rows); });
+    TIGRE_CUDA(cudaGetLastError());
+    return TIGRE_SUCCESS;
+}
 
 int launch_make_layout(const void* src, int dtype, void* dst, int nX, int nY, int nZ, int layout, int pad_lo,
                        int pad_hi, cudaStream_t st) {

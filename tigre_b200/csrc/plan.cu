@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <cstdio>
 #include <cstdlib>
 #include <mutex>
 
@@ -213,6 +214,80 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
     }
     plan->axial = axial;
     plan->columns = columns && std::getenv("TIGRE_B200_GENERIC_SIDDON") == nullptr;
+
+    // ---- staged backprojector constants and patch box ----
+    plan->h_bpk.resize(nangles);
+    double ext_u = 0.0, ext_v = 0.0;
+    const int bx = 16, bz = 16;
+    for (int i = 0; i < nangles; ++i) {
+        const FrameBP& f = plan->h_bp[i];
+        FrameBPK& k = plan->h_bpk[i];
+        for (int c = 0; c < 3; ++c) { k.dx[c] = f.dx[c]; k.dy[c] = f.dy[c]; k.dz[c] = f.dz[c]; }
+        k.b[0] = f.o[0] - f.s[0];
+        k.b[1] = f.o[1] - (double)f.cor / d.dDU - f.s[1];
+        k.b[2] = f.o[2] - f.s[2];
+        k.tnum = (float)((double)f.dso - (double)f.dsd - f.s[0]);
+        k.cu = (float)(f.s[1] + d.nU * 0.5);
+        k.cv = (float)(f.s[2] + d.nV * 0.5);
+        const double sina = f.sina, cosa = f.cosa;
+        k.w0 = (float)(f.dso + (-(d.sVY - d.dVY) * 0.5 + f.offy + f.cor) * sina - (-(d.sVX - d.dVX) * 0.5 + f.offx) * cosa);
+        k.wx = (float)(-d.dVX * cosa);
+        k.wy = (float)(d.dVY * sina);
+        k.dso = f.dso;
+        k.dsd = f.dsd;
+        k.rsx = (float)(f.dso * cosa);
+        k.rsy = (float)(-f.dso * sina);
+        const double dax = -((double)f.dsd - (double)f.dso);
+        k.daxc = (float)(dax * cosa);
+        k.daxs = (float)(dax * sina);
+        k.sina = f.sina;
+        k.cosa = f.cosa;
+        k.du0 = (float)((-d.sDU + d.dDU) * 0.5 + f.offu);
+        k.ddu = (float)d.dDU;
+        k.dzc = (float)((-d.sDV + d.dDV) * 0.5 + f.offv);
+        k.ddv = (float)d.dDV;
+        k.rv0x = (float)(-d.sVX / 2 + d.dVX / 2 + f.offx);
+        k.rv0y = (float)(-d.sVY / 2 + d.dVY / 2 + f.offy);
+        k.rv0z = (float)(-d.sVZ / 2 + d.dVZ / 2 + f.offz);
+        k.dvx = (float)d.dVX;
+        k.dvy = (float)d.dVY;
+        // footprint of sample blocks (first / middle / last along each axis) for this view
+        const int nbx = (d.nX + bx - 1) / bx, nby = (d.nY + bx - 1) / bx, nbz = (d.nZ + bz - 1) / bz;
+        const int sx[3] = {0, nbx / 2, nbx - 1}, sy[3] = {0, nby / 2, nby - 1}, sz[3] = {0, nbz / 2, nbz - 1};
+        for (int ix = 0; ix < 3; ++ix)
+            for (int iy = 0; iy < 3; ++iy)
+                for (int iz = 0; iz < 3; ++iz) {
+                    double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
+                    for (int c = 0; c < 8; ++c) {
+                        const double x = std::min(sx[ix] * bx + ((c & 1) ? bx - 1 : 0), d.nX - 1);
+                        const double y = std::min(sy[iy] * bx + ((c & 2) ? bx - 1 : 0), d.nY - 1);
+                        const double z = std::min(sz[iz] * bz + ((c & 4) ? bz - 1 : 0), d.nZ - 1);
+                        const double vx = k.b[0] + x * k.dx[0] + y * k.dy[0] + z * k.dz[0];
+                        const double vy = k.b[1] + x * k.dx[1] + y * k.dy[1] + z * k.dz[1];
+                        const double vz = k.b[2] + x * k.dx[2] + y * k.dy[2] + z * k.dz[2];
+                        const double t = (double)k.tnum / vx;
+                        const double u = vy * t, v = vz * t;
+                        umin = std::min(umin, u); umax = std::max(umax, u);
+                        vmin = std::min(vmin, v); vmax = std::max(vmax, v);
+                    }
+                    ext_u = std::max(ext_u, umax - umin);
+                    ext_v = std::max(ext_v, vmax - vmin);
+                }
+    }
+    {
+        int BU = ((int)std::ceil(ext_u) + 13 + 7) / 8 * 8;
+        int BV = (int)std::ceil(ext_v) + 6;
+        if (BU < 8) BU = 8;
+        if (BV < 4) BV = 4;
+        if (const char* ov = std::getenv("TIGRE_B200_BP_BOX")) {   // test hook: force a box (e.g. "8x4")
+            int bu = 0, bv = 0;
+            if (std::sscanf(ov, "%dx%d", &bu, &bv) == 2 && bu > 0 && bv > 0) { BU = (bu + 7) / 8 * 8; BV = bv; }
+        }
+        const bool ok = std::isfinite(ext_u) && std::isfinite(ext_v) && BU <= 256 && BV <= 256 &&
+                        2.0 * BU * BV * 4 <= 96.0 * 1024 && std::getenv("TIGRE_B200_NO_TMA") == nullptr;
+        plan->bp_box_u = ok ? BU : 0;
+        plan->bp_box_v = ok ? BV : 0;
+    }
     return TIGRE_SUCCESS;
 }
 
@@ -258,8 +333,13 @@ int tigre_plan_create(const TigreGeometry* geo, const float* angles, int nangles
     cudaGetDevice(&prev);
     cudaSetDevice(device);
     const size_t ns = sizeof(FrameSiddon) * nangles, ni = sizeof(FrameInterp) * nangles, nb = sizeof(FrameBP) * nangles;
+    const size_t nk = sizeof(FrameBPK) * nangles;
     e = cudaMalloc(&p->d_siddon, ns);
     if (e == cudaSuccess) e = cudaMalloc(&p->d_interp, ni);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_bpk, nk);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(p->d_status, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_bpk, p->h_bpk.data(), nk, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&p->d_bp, nb);
     if (e == cudaSuccess) e = cudaMemcpy(p->d_siddon, p->h_siddon.data(), ns, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(p->d_interp, p->h_interp.data(), ni, cudaMemcpyHostToDevice);
@@ -282,10 +362,24 @@ void tigre_plan_destroy(TigrePlan* p) {
     cudaFree(p->d_siddon);
     cudaFree(p->d_interp);
     cudaFree(p->d_bp);
+    cudaFree(p->d_bpk);
+    cudaFree(p->d_status);
     cudaSetDevice(prev);
     delete p;
 }
 
 long long tigre_plan_scratch_bytes(const TigrePlan* p) { return p ? (long long)p->scratch_bytes : 0; }
+
+int tigre_plan_status(TigrePlan* p, int reset) {
+    if (!p) return -1;
+    int prev = 0, v = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(p->device);
+    cudaDeviceSynchronize();
+    cudaMemcpy(&v, p->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (reset) cudaMemset(p->d_status, 0, sizeof(int));
+    cudaSetDevice(prev);
+    return v;
+}
 
 }  // extern "C"

@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(256) siddon_count_kernel(SiddonArgs p) {
 // (column groups fastest, then views, then row tiles) keeps the z-slab of the
 // current row tile L2-resident while every view is processed.
 template <typename TV, typename TP, int R>
-__global__ void __launch_bounds__(128) siddon_columns_kernel(SiddonArgs p) {
+__global__ void __launch_bounds__(128, 6) siddon_columns_kernel(SiddonArgs p) {
     const int lane = threadIdx.x & 31;
     const int u = blockIdx.x * 4 + (threadIdx.x >> 5);
     const int la = blockIdx.y;
@@ -283,40 +283,52 @@ __global__ void __launch_bounds__(128) siddon_columns_kernel(SiddonArgs p) {
     int remx = ax.rem, remy = ay.rem;
     float tx = ax.t0, ty = ay.t0, kx = 0.f, ky = 0.f;
     float a = 0.f;
+    // value of each row's current voxel in the current cell, loaded one cell ahead
+    float vcur[R];
+    {
+        const TV* col = vol + cidx * ZP + 1;
+#pragma unroll
+        for (int r = 0; r < R; ++r) vcur[r] = ldg_f<TV>(col + iz[r]);
+    }
 #pragma unroll 1
     for (int c = 0; c < ncells; ++c) {
         const float tn = fminf(tx, ty);
         const float b = fminf(tn, T);
+        const float seg = b - a;
         const TV* col = vol + cidx * ZP + 1;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            float val = ldg_f<TV>(col + iz[r]);
-            if (tz[r] < b) {
-                // z crossings inside this cell (rare at cone-beam angles)
-                float st = a;
+            // no-crossing contribution; a z crossing at tz inside the cell adds
+            // (b - tz) * (v_after - v_before) (branch-free for the usual single crossing)
+            sum[r] = fmaf(seg, vcur[r], sum[r]);
+            const bool cross = tz[r] < b;
+            if (cross) {
+                float vb = vcur[r];
                 do {
-                    sum[r] = fmaf(tz[r] - st, val, sum[r]);
-                    st = tz[r];
                     iz[r] += sz[r];
+                    const float vn = ldg_f<TV>(col + iz[r]);
+                    sum[r] = fmaf(b - tz[r], vn - vb, sum[r]);
+                    vb = vn;
                     kz[r] += 1.f;
                     const bool more = sz[r] > 0 ? iz[r] < p.nZ : iz[r] >= 0;
                     tz[r] = more ? fmaf(kz[r], dtz[r], tz0[r]) : kInf;
-                    val = ldg_f<TV>(col + iz[r]);
                 } while (tz[r] < b);
-                sum[r] = fmaf(b - st, val, sum[r]);
-            } else {
-                sum[r] = fmaf(b - a, val, sum[r]);
             }
         }
         a = b;
-        if (tx <= ty) {
-            cidx += dcx;
+        const bool stepx = tx <= ty;
+        cidx += stepx ? dcx : dcy;
+        if (stepx) {
             kx += 1.f;
             tx = (--remx > 0) ? fmaf(kx, ax.dt, ax.t0) : kInf;
         } else {
-            cidx += dcy;
             ky += 1.f;
             ty = (--remy > 0) ? fmaf(ky, ay.dt, ay.t0) : kInf;
+        }
+        if (c + 1 < ncells) {
+            const TV* nc = vol + cidx * ZP + 1;
+#pragma unroll
+            for (int r = 0; r < R; ++r) vcur[r] = ldg_f<TV>(nc + iz[r]);
         }
     }
 #pragma unroll

@@ -64,6 +64,23 @@ struct FrameBP {
     float offu, offv;         // offDetec
 };
 
+// Per-view constants of the staged backprojector (backproject_tma.cu), derived from
+// FrameBP on the host so that a (column, view) needs only FMAs and one division.
+struct FrameBPK {
+    double b[3];             // voxel (0,0,0) minus source, y shifted by -COR/dDetecU
+    double dx[3], dy[3], dz[3];
+    float tnum;              // DSO - DSD - S.x
+    float cu, cv;            // texture-coordinate offsets S.y + nU/2, S.z + nV/2
+    float w0, wx, wy;        // FDK: U = w0 + x wx + y wy, weight (DSO/U)^2
+    float dso, dsd;
+    float rsx, rsy;          // matched: source position (mm)
+    float daxc, daxs;        // -(DSD-DSO) cos a, -(DSD-DSO) sin a
+    float sina, cosa;
+    float du0, ddu, dzc, ddv;
+    float rv0x, rv0y, rv0z;  // voxel (0,0,0) centre in mm (with offOrig)
+    float dvx, dvy;
+};
+
 struct Plan;
 
 // ----------------------------------------------------------------- plan ---
@@ -89,6 +106,10 @@ struct TigrePlan {
     tigre::FrameBP* d_bp = nullptr;
     bool axial = false;          // every BP frame has dz.x == dz.y == 0 (u constant along z)
     bool columns = false;        // every Siddon frame has dv.x == dv.y == 0 (detector v parallel to z)
+    std::vector<tigre::FrameBPK> h_bpk;
+    tigre::FrameBPK* d_bpk = nullptr;
+    int bp_box_u = 0, bp_box_v = 0;   // TMA patch box of the staged backprojector (0: not usable)
+    int* d_status = nullptr;          // kernel error word (bounded waits that expired)
     // growable stream-ordered scratch arena
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -114,6 +135,12 @@ int launch_interp(TigrePlan* p, const void* vol_x, const void* vol_y, int vdt, v
                   cudaStream_t st);
 int launch_backproject(TigrePlan* p, const void* proj_pad, int pdt, void* vol, int vdt, int matched, int a0, int a1,
                        cudaStream_t st);
+
+bool bp_tma_supported(const TigrePlan* p, int pdt);
+int launch_backproject_tma(TigrePlan* p, const void* proj, int pitch, int pdt, void* vol, int vdt, int matched,
+                           int a0, int a1, cudaStream_t st);
+int launch_repitch_projections(const void* src, int dtype, void* dst, int nA, int nV, int nU, int pitch,
+                               cudaStream_t st);
 
 // padded projection pitch and row count used by the backprojector
 __host__ __device__ inline long bp_pitch(int nU) { return (long)nU + 3; }
