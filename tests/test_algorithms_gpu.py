@@ -106,33 +106,53 @@ def test_autograd_backward_is_matched_adjoint():
 
 
 def test_autograd_loss_finite_differences():
-    """loss = |Ax - b|^2 + 1e-3 TV(x): autograd vs central differences (h = 1e-3).
-    The backward of Ax is the matched backprojector, the reference's approximate
-    adjoint of Siddon, so agreement is within its adjoint gap (a few %)."""
+    """loss = |Ax - b|^2 + 1e-3 TV(x), central differences at h = 1e-3 along directions d.
+
+    * TV term (hand-written backward): exact, checked along random directions;
+    * data term: the backward of Ax is the matched backprojector, the reference's
+      approximate adjoint of Siddon -- per voxel it differs for rough data, so the
+      check is along smooth directions (Gaussian blobs), within the adjoint gap (3%)."""
     import torch
     from tigre_b200 import autograd as AG
     geo, ang, img = _case(n=24, views=18)
     rng = np.random.default_rng(0)
     A = AG.A(geo, ang)
     b = torch.from_numpy(O.ax(img, geo, ang, "Siddon")).cuda().double()
-    # noise >> h keeps every |grad f| term of the TV away from its kink during the differences
     x0 = torch.from_numpy((img + rng.normal(0, 5e-2, img.shape)).astype(np.float32)).cuda()
+    h = 1e-3
+
+    def data(x):
+        r = A(x).double() - b
+        return (r * r).sum()
+
+    def tvl(x):
+        return AG.tv(x).double()
 
     def loss(x):
-        r = A(x).double() - b
-        return (r * r).sum() + 1e-3 * AG.tv(x).double()
+        return data(x) + 1e-3 * tvl(x)
 
-    x = x0.clone().requires_grad_(True)
-    loss(x).backward()
-    g = x.grad.double()
-    h = 1e-3
-    errs = []
-    for idx in [(12, 12, 12), (8, 15, 10), (16, 6, 9)]:
-        xp = x0.clone(); xp[idx] += h
-        xm = x0.clone(); xm[idx] -= h
-        fd = (loss(xp) - loss(xm)).item() / (2 * h)
-        errs.append(abs(fd - g[idx].item()) / max(abs(fd), 1e-12))
-    assert max(errs) < 0.05, errs
+    def grad(f):
+        x = x0.clone().requires_grad_(True)
+        f(x).backward()
+        return x.grad.double()
+
+    def fd(f, d):
+        return (f(x0 + h * d) - f(x0 - h * d)).item() / (2 * h)
+
+    zz, yy, xx = np.meshgrid(*[np.arange(24)] * 3, indexing="ij")
+    blobs = []
+    for c in [(12, 12, 12), (8, 15, 10), (16, 6, 9)]:
+        blob = np.exp(-((zz - c[0]) ** 2 + (yy - c[1]) ** 2 + (xx - c[2]) ** 2) / (2 * 3.0 ** 2))
+        blobs.append(torch.from_numpy(blob.astype(np.float32)).cuda())
+    g_data, g_tv, g_all = grad(data), grad(tvl), grad(loss)
+    for d in blobs:
+        e_data = abs(fd(data, d) - (g_data * d).sum().item()) / abs(fd(data, d))
+        e_all = abs(fd(loss, d) - (g_all * d).sum().item()) / abs(fd(loss, d))
+        assert e_data < 0.03 and e_all < 0.03, (e_data, e_all)
+    for seed in range(3):
+        d = torch.from_numpy(np.random.default_rng(seed).normal(0, 1, img.shape).astype(np.float32)).cuda()
+        ref = fd(tvl, d)
+        assert abs(ref - (g_tv * d).sum().item()) <= 1e-3 * abs(ref), (seed, ref)
 
 
 def test_autograd_batch_dimension():
