@@ -68,6 +68,26 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
     return false;
 }
 
+template <typename TP> __device__ __forceinline__ float lds(uint32_t a);
+template <> __device__ __forceinline__ float lds<float>(uint32_t a) {
+    float v;
+    asm("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+    return v;
+}
+template <> __device__ __forceinline__ float lds<__nv_bfloat16>(uint32_t a) {
+    unsigned short v;
+    asm("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(a));
+    return __uint_as_float(((unsigned)v) << 16);
+}
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+// a + t (b - a), two lanes at once
+__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 t) {
+    return __ffma2_rn(t, __fadd2_rn(b, neg2(a)), a);
+}
+
 // texel-space (u - 0.5, v - 0.5) projection of voxel (x, y, z) for view frame F
 __device__ __forceinline__ void project_texel(const FrameBPK& F, float x, float y, float z, float& ub, float& vb) {
     const double vx = fma((double)z, F.dz[0], fma((double)y, F.dy[0], fma((double)x, F.dx[0], F.b[0])));
@@ -165,6 +185,8 @@ __global__ void __launch_bounds__(TXY* TXY) bp_tma_kernel(const __grid_constant_
     const size_t buf_bytes = ((size_t)p.BU * p.BV * sizeof(TP) + 127) / 128 * 128;
     TP* buf0 = reinterpret_cast<TP*>(smem_raw + base_off);
     TP* buf1 = reinterpret_cast<TP*>(smem_raw + base_off + buf_bytes);
+    const uint32_t buf0_u32 = smem_u32(buf0), buf1_u32 = smem_u32(buf1);
+    const uint32_t rowb = (uint32_t)(p.BU * sizeof(TP));
     const int tid = threadIdx.x;
     const int tx = tid & (TXY - 1), ty = tid / TXY;
     const int x0 = blockIdx.x * TXY, y0 = blockIdx.y * TXY, z0 = blockIdx.z * VZ;
@@ -193,6 +215,7 @@ __global__ void __launch_bounds__(TXY* TXY) bp_tma_kernel(const __grid_constant_
         // after one expired wait the block stops waiting (its result is flagged invalid)
         if (!failed && !mbar_wait(bar, (uint32_t)((la >> 1) & 1))) failed = true;
         const TP* patch = s ? buf1 : buf0;
+        const uint32_t patch_u32 = s ? buf1_u32 : buf0_u32;
         const int u0 = info[s][0], v0 = info[s][1], fits = info[s][2];
         if (active) {
             const FrameBPK& F = p.frames[p.a0 + la];
@@ -222,22 +245,47 @@ __global__ void __launch_bounds__(TXY* TXY) bp_tma_kernel(const __grid_constant_
                 if (fits) {
                     const float pu = fminf(fmaxf(u - 0.5f - (float)u0, 0.f), pumax);
                     const int iu = (int)pu;
-                    const float fu = pu - (float)iu;
+                    const float2 fu2 = f2(pu - (float)iu);
                     const float pv0 = vt0 - 0.5f - (float)v0;
+                    constexpr uint32_t ES = (uint32_t)sizeof(TP);
+                    const uint32_t colb = patch_u32 + (uint32_t)iu * ES;
+                    const float2 vstep2 = f2(vstep);
+                    const float2 pv02 = f2(pv0);
+                    float2 vt02 = f2(0.f), dzc2 = f2(0.f), ddv2 = f2(0.f), cu22 = f2(0.f), cxy2 = f2(0.f);
+                    float2 dvz2 = f2(0.f), rz2 = f2(0.f), dsd2 = f2(0.f);
+                    if (MATCHED) {
+                        vt02 = f2(vt0); dzc2 = f2(F.dzc); ddv2 = f2(F.ddv); cu22 = f2(cu2); cxy2 = f2(cxy);
+                        dvz2 = f2(p.dVZ); rz2 = f2(fmaf((float)z0, p.dVZ, F.rv0z)); dsd2 = f2(F.dsd);
+                    }
+                    const float2 w2 = f2(wcol);
 #pragma unroll
-                    for (int k = 0; k < VZ; ++k) {
-                        const float smp = patch_sample<TP>(patch, p.BU, iu, fu, fmaf((float)k, vstep, pv0), pvmax);
-                        if (!MATCHED) {
-                            acc[k] = fmaf(smp, wcol, acc[k]);
-                        } else {
-                            const float vtex = fmaf((float)k, vstep, vt0);
-                            const float dz = fmaf(vtex, F.ddv, F.dzc);
-                            const float L2 = fmaf(dz, dz, cu2);
-                            const float rvz = fmaf((float)(z0 + k), p.dVZ, F.rv0z);
-                            const float lsq = fmaf(rvz, rvz, cxy);
-                            const float w = L2 * (L2 * rsqrtf(L2)) * __frcp_rn(F.dsd * lsq);
-                            acc[k] = fmaf(smp, w, acc[k]);
+                    for (int k = 0; k < VZ; k += 2) {
+                        const float2 kk = f2((float)k, (float)(k + 1));
+                        float2 pv = __ffma2_rn(kk, vstep2, pv02);
+                        pv.x = fminf(fmaxf(pv.x, 0.f), pvmax);
+                        pv.y = fminf(fmaxf(pv.y, 0.f), pvmax);
+                        const int ia = (int)pv.x, ib = (int)pv.y;
+                        const float2 fv = __fadd2_rn(pv, f2(-(float)ia, -(float)ib));
+                        const uint32_t aa = colb + (uint32_t)ia * rowb, ab = colb + (uint32_t)ib * rowb;
+                        const float2 r0 = f2(lds<TP>(aa), lds<TP>(ab)), r0r = f2(lds<TP>(aa + ES), lds<TP>(ab + ES));
+                        const float2 r1 = f2(lds<TP>(aa + rowb), lds<TP>(ab + rowb));
+                        const float2 r1r = f2(lds<TP>(aa + rowb + ES), lds<TP>(ab + rowb + ES));
+                        const float2 smp = lerp2(lerp2(r0, r0r, fu2), lerp2(r1, r1r, fu2), fv);
+                        float2 w = w2;
+                        if (MATCHED) {
+                            const float2 vtex = __ffma2_rn(kk, vstep2, vt02);
+                            const float2 dz = __ffma2_rn(vtex, ddv2, dzc2);
+                            const float2 L2 = __ffma2_rn(dz, dz, cu22);
+                            const float2 rvz = __ffma2_rn(kk, dvz2, rz2);
+                            const float2 lsq = __ffma2_rn(rvz, rvz, cxy2);
+                            const float2 rs = f2(rsqrtf(L2.x), rsqrtf(L2.y));
+                            const float2 L3 = __fmul2_rn(L2, __fmul2_rn(L2, rs));
+                            const float2 den = __fmul2_rn(lsq, dsd2);
+                            w = __fmul2_rn(L3, f2(__fdividef(1.f, den.x), __fdividef(1.f, den.y)));
                         }
+                        const float2 acc2 = __ffma2_rn(smp, w, f2(acc[k], acc[k + 1]));
+                        acc[k] = acc2.x;
+                        acc[k + 1] = acc2.y;
                     }
                 } else {
 #pragma unroll 1

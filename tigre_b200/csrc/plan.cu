@@ -276,6 +276,7 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
     }
     {
         int BU = ((int)std::ceil(ext_u) + 13 + 7) / 8 * 8;
+        while (BU % 32 != 8) BU += 8;   // row pitch = 8 banks mod 32: neighbouring rows do not collide
         int BV = (int)std::ceil(ext_v) + 6;
         if (BU < 8) BU = 8;
         if (BV < 4) BV = 4;

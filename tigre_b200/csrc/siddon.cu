@@ -296,23 +296,38 @@ __global__ void __launch_bounds__(128, 6) siddon_columns_kernel(SiddonArgs p) {
         const float b = fminf(tn, T);
         const float seg = b - a;
         const TV* col = vol + cidx * ZP + 1;
+        bool again = false;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             // no-crossing contribution; a z crossing at tz inside the cell adds
-            // (b - tz) * (v_after - v_before) (branch-free for the usual single crossing)
+            // (b - tz) * (v_after - v_before).  The first crossing is handled by a short
+            // predicated body; z indices are clamped to the zero pads [-1, nZ], so a ray
+            // that has left the volume keeps crossing planes at no cost and reads 0.
             sum[r] = fmaf(seg, vcur[r], sum[r]);
-            const bool cross = tz[r] < b;
-            if (cross) {
-                float vb = vcur[r];
-                do {
-                    iz[r] += sz[r];
-                    const float vn = ldg_f<TV>(col + iz[r]);
-                    sum[r] = fmaf(b - tz[r], vn - vb, sum[r]);
-                    vb = vn;
+            if (tz[r] < b) {
+                const int izn = min(max(iz[r] + sz[r], -1), p.nZ);
+                const float vn = ldg_f<TV>(col + izn);
+                sum[r] = fmaf(b - tz[r], vn - vcur[r], sum[r]);
+                vcur[r] = vn;
+                iz[r] = izn;
+                kz[r] += 1.f;
+                tz[r] = fmaf(kz[r], dtz[r], tz0[r]);
+                again |= tz[r] < b;
+            }
+        }
+        if (__any_sync(0xffffffffu, again)) {
+            // steep rays: further crossings inside the same cell (warp-uniform, rare)
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                while (tz[r] < b) {
+                    const int izn = min(max(iz[r] + sz[r], -1), p.nZ);
+                    const float vn = ldg_f<TV>(col + izn);
+                    sum[r] = fmaf(b - tz[r], vn - vcur[r], sum[r]);
+                    vcur[r] = vn;
+                    iz[r] = izn;
                     kz[r] += 1.f;
-                    const bool more = sz[r] > 0 ? iz[r] < p.nZ : iz[r] >= 0;
-                    tz[r] = more ? fmaf(kz[r], dtz[r], tz0[r]) : kInf;
-                } while (tz[r] < b);
+                    tz[r] = fmaf(kz[r], dtz[r], tz0[r]);
+                }
             }
         }
         a = b;
