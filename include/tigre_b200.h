@@ -154,6 +154,14 @@ int tigre_ax(TigrePlan* plan, const void* d_vol, int vol_dtype, void* d_proj, in
 int tigre_atb(TigrePlan* plan, const void* d_proj, int proj_dtype, void* d_vol, int vol_dtype, int backprojector,
               int angle_begin, int angle_end, void* stream);
 
+/* As tigre_atb; accumulate != 0 adds into d_vol instead of overwriting it (lets a caller
+ * stream the views in chunks). */
+int tigre_atb_ex(TigrePlan* plan, const void* d_proj, int proj_dtype, void* d_vol, int vol_dtype, int backprojector,
+                 int angle_begin, int angle_end, int accumulate, void* stream);
+
+/* Frees the device buffers and plans that the host entry points keep between calls. */
+void tigre_release_cache(void);
+
 /* Sum over all rays of the number of Siddon voxel segments (FP64 ray setup only,
  * no traversal); the algorithmic-bytes count of the Siddon roofline. */
 int tigre_siddon_count_segments(TigrePlan* plan, int angle_begin, int angle_end, unsigned long long* d_total,

@@ -26,6 +26,12 @@ def tilted_geometry():
     return g
 
 
+def steep_geometry():
+    """Short source distance and 0.25 mm slices: rays climb up to ~1.5 slices per xy cell,
+    so the column projector takes its several-crossings-per-cell path."""
+    return cone_geometry((40, 48, 48), (10.0, 48.0, 48.0), (128, 96), (1.5, 1.5), DSO=150.0, DSD=250.0)
+
+
 def angles(n, full=2 * np.pi, tilt=False, seed=3):
     a = np.linspace(0, full, n, endpoint=False).astype(np.float32)
     if not tilt:

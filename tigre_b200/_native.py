@@ -78,6 +78,9 @@ _SIGS = {
                            C.c_void_p]),
     "tigre_atb": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                             C.c_void_p]),
+    "tigre_atb_ex": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                               C.c_int, C.c_void_p]),
+    "tigre_release_cache": (None, []),
     "tigre_siddon_count_segments": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "tigre_tv_pocs": (C.c_int, [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_int, C.c_void_p,
                                 C.c_void_p]),
@@ -229,3 +232,18 @@ def get_plan(geo_checked, device=0) -> Plan:
 
 def clear_plan_cache():
     _plan_cache.clear()
+
+
+def host_empty(shape):
+    """float32 numpy array for a host-path result, in page-locked memory when a
+    GPU is present (device->host copies into pageable memory go through a
+    driver bounce buffer at a fraction of the link rate).  The pages come from
+    torch's caching host allocator, so repeated calls of one size reuse them;
+    the array keeps its tensor alive."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return torch.empty(tuple(shape), dtype=torch.float32, pin_memory=True).numpy()
+    except ImportError:
+        pass
+    return np.empty(tuple(shape), dtype=np.float32)

@@ -93,6 +93,11 @@ int tigre_ax(TigrePlan* plan, const void* d_vol, int vdt, void* d_proj, int pdt,
 
 int tigre_atb(TigrePlan* plan, const void* d_proj, int pdt, void* d_vol, int vdt, int backprojector, int a0, int a1,
               void* stream) {
+    return tigre_atb_ex(plan, d_proj, pdt, d_vol, vdt, backprojector, a0, a1, 0, stream);
+}
+
+int tigre_atb_ex(TigrePlan* plan, const void* d_proj, int pdt, void* d_vol, int vdt, int backprojector, int a0, int a1,
+                 int accumulate, void* stream) {
     if (int rc = check_range(plan, a0, a1)) return rc;
     if (!d_vol || !d_proj) return fail(TIGRE_ERR_BAD_ASSERT, "null device pointer");
     if (!dtype_ok(vdt) || !dtype_ok(pdt)) return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype");
@@ -107,18 +112,19 @@ int tigre_atb(TigrePlan* plan, const void* d_proj, int pdt, void* d_vol, int vdt
         const int align = 16 / (int)dtype_size(pdt);
         if (d.nU % align == 0 && ((uintptr_t)d_proj % 16) == 0)
             return launch_backproject_tma(plan, d_proj, d.nU, pdt, d_vol, vdt,
-                                          backprojector == TIGRE_BACKPROJ_MATCHED, a0, a1, st);
+                                          backprojector == TIGRE_BACKPROJ_MATCHED, a0, a1, accumulate, st);
         const int pitch = (d.nU + align - 1) / align * align;
         void* s = plan_scratch(plan, (size_t)na * d.nV * pitch * dtype_size(pdt), st, &rc);
         if (rc) return rc;
         if ((rc = launch_repitch_projections(d_proj, pdt, s, na, d.nV, d.nU, pitch, st))) return rc;
         return launch_backproject_tma(plan, s, pitch, pdt, d_vol, vdt, backprojector == TIGRE_BACKPROJ_MATCHED, a0,
-                                      a1, st);
+                                      a1, accumulate, st);
     }
     void* s = plan_scratch(plan, (size_t)na * bp_rows(d.nV) * bp_pitch(d.nU) * dtype_size(pdt), st, &rc);
     if (rc) return rc;
     if ((rc = launch_pad_projections(d_proj, pdt, s, na, d.nV, d.nU, st))) return rc;
-    return launch_backproject(plan, s, pdt, d_vol, vdt, backprojector == TIGRE_BACKPROJ_MATCHED, a0, a1, st);
+    return launch_backproject(plan, s, pdt, d_vol, vdt, backprojector == TIGRE_BACKPROJ_MATCHED, a0, a1, accumulate,
+                              st);
 }
 
 int tigre_siddon_count_segments(TigrePlan* plan, int a0, int a1, unsigned long long* d_total, void* stream) {
@@ -131,6 +137,12 @@ int tigre_siddon_count_segments(TigrePlan* plan, int a0, int a1, unsigned long l
 }  // extern "C"
 
 // ---------------------------------------------------------------- host API --
+//
+// Per device, the host entry points keep (a) the plans of the last few
+// geometries, keyed by the bytes of the geometry and the angles, and (b) a
+// small set of device buffers that only grow, so repeated calls on the same
+// geometry allocate nothing and recompute no frames.  Calls on one device are
+// serialised (the reference's host functions are not reentrant either).
 
 namespace {
 
@@ -143,28 +155,104 @@ int pick_device(const int* ids, int n, int* dev) {
     return TIGRE_SUCCESS;
 }
 
-struct HostCall {
-    TigrePlan* plan = nullptr;
-    cudaStream_t st = nullptr, st2 = nullptr;
-    cudaEvent_t ev[2] = {nullptr, nullptr};
-    std::vector<void*> bufs;
-    ~HostCall() {
-        if (st) cudaStreamSynchronize(st);
-        if (st2) cudaStreamSynchronize(st2);
-        for (void* b : bufs) cudaFree(b);
-        for (auto& e : ev)
-            if (e) cudaEventDestroy(e);
-        if (st) cudaStreamDestroy(st);
-        if (st2) cudaStreamDestroy(st2);
-        if (plan) tigre_plan_destroy(plan);
+uint64_t fnv(uint64_t h, const void* p, size_t n) {
+    const unsigned char* c = (const unsigned char*)p;
+    for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ull;
+    return h;
+}
+
+uint64_t geometry_key(const TigreGeometry* g, const float* angles, int n) {
+    uint64_t h = 1469598103934665603ull;
+    TigreGeometry s = *g;
+    const float* arrays[] = {g->offOrigX, g->offOrigY, g->offOrigZ, g->DSO, g->offDetecU, g->offDetecV,
+                             g->DSD, g->dRoll, g->dPitch, g->dYaw, g->COR};
+    s.offOrigX = s.offOrigY = s.offOrigZ = s.DSO = s.offDetecU = s.offDetecV = s.DSD = nullptr;
+    s.dRoll = s.dPitch = s.dYaw = s.COR = nullptr;
+    h = fnv(h, &s, sizeof(s));
+    for (const float* a : arrays) {
+        const unsigned char present = a != nullptr;
+        h = fnv(h, &present, 1);
+        if (a) h = fnv(h, a, sizeof(float) * (size_t)n);
     }
-    int alloc(void** p, size_t bytes) {
-        cudaError_t e = cudaMalloc(p, bytes);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
-        bufs.push_back(*p);
+    h = fnv(h, angles, sizeof(float) * 3 * (size_t)n);
+    return fnv(h, &n, sizeof(n));
+}
+
+struct DeviceState {
+    std::mutex mu;
+    cudaStream_t st = nullptr, st2 = nullptr;
+    cudaEvent_t ev[4] = {};
+    void* buf[4] = {};
+    size_t bytes[4] = {};
+    struct Entry { uint64_t key; TigrePlan* plan; };
+    std::vector<Entry> plans;
+
+    int init(int dev) {
+        if (st) return TIGRE_SUCCESS;
+        TIGRE_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        TIGRE_CUDA(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+        for (auto& e : ev) TIGRE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        (void)dev;
         return TIGRE_SUCCESS;
     }
+    int get(int slot, size_t n, void** out) {
+        if (bytes[slot] < n) {
+            if (buf[slot]) {
+                cudaStreamSynchronize(st);
+                cudaStreamSynchronize(st2);
+                cudaFree(buf[slot]);
+                buf[slot] = nullptr;
+                bytes[slot] = 0;
+            }
+            TIGRE_CUDA(cudaMalloc(&buf[slot], n));
+            bytes[slot] = n;
+        }
+        *out = buf[slot];
+        return TIGRE_SUCCESS;
+    }
+    int plan(const TigreGeometry* g, const float* angles, int n, int dev, TigrePlan** out) {
+        const uint64_t k = geometry_key(g, angles, n);
+        for (auto& e : plans)
+            if (e.key == k) { *out = e.plan; return TIGRE_SUCCESS; }
+        TigrePlan* p = nullptr;
+        if (int rc = tigre_plan_create(g, angles, n, dev, &p)) return rc;
+        if (plans.size() >= 4) {
+            cudaStreamSynchronize(st);
+            tigre_plan_destroy(plans.front().plan);
+            plans.erase(plans.begin());
+        }
+        plans.push_back({k, p});
+        *out = p;
+        return TIGRE_SUCCESS;
+    }
+    void release() {
+        if (st) { cudaStreamSynchronize(st); cudaStreamSynchronize(st2); }
+        for (auto& e : plans) tigre_plan_destroy(e.plan);
+        plans.clear();
+        for (int i = 0; i < 4; ++i) {
+            if (buf[i]) cudaFree(buf[i]);
+            buf[i] = nullptr;
+            bytes[i] = 0;
+        }
+    }
 };
+
+std::mutex g_states_mu;
+std::vector<DeviceState*> g_states;
+
+DeviceState* state(int dev) {
+    std::lock_guard<std::mutex> lk(g_states_mu);
+    if ((int)g_states.size() <= dev) g_states.resize(dev + 1, nullptr);
+    if (!g_states[dev]) g_states[dev] = new DeviceState();
+    return g_states[dev];
+}
+
+// Views per host<->device chunk: ~192 MB of projections, or TIGRE_B200_HOST_CHUNK_VIEWS.
+size_t chunk_views(size_t per_view_bytes, int nangles) {
+    size_t c = ((size_t)192 << 20) / std::max<size_t>(per_view_bytes, 1);
+    if (const char* e = getenv("TIGRE_B200_HOST_CHUNK_VIEWS")) c = (size_t)std::max(1, atoi(e));
+    return std::max<size_t>(1, std::min<size_t>((size_t)nangles, c));
+}
 
 int host_project(const float* img, const TigreGeometry* geo, float* const* result, const float* angles, int nangles,
                  const int* ids, int n, int projector) {
@@ -172,51 +260,36 @@ int host_project(const float* img, const TigreGeometry* geo, float* const* resul
     int dev = 0;
     if (int rc = pick_device(ids, n, &dev)) return rc;
     DeviceGuard g(dev);
-    HostCall h;
-    if (int rc = tigre_plan_create(geo, angles, nangles, dev, &h.plan)) return rc;
-    const Dims& d = h.plan->d;
-    TIGRE_CUDA(cudaStreamCreateWithFlags(&h.st, cudaStreamNonBlocking));
-    TIGRE_CUDA(cudaStreamCreateWithFlags(&h.st2, cudaStreamNonBlocking));
-    for (auto& e : h.ev) TIGRE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    DeviceState* S = state(dev);
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (int rc = S->init(dev)) return rc;
+    TigrePlan* plan = nullptr;
+    if (int rc = S->plan(geo, angles, nangles, dev, &plan)) return rc;
+    const Dims& d = plan->d;
     const size_t nvox = (size_t)d.nX * d.nY * d.nZ, npix = (size_t)d.nU * d.nV;
     void* dvol = nullptr;
-    if (int rc = h.alloc(&dvol, nvox * sizeof(float))) return rc;
-    TIGRE_CUDA(cudaMemcpyAsync(dvol, img, nvox * sizeof(float), cudaMemcpyHostToDevice, h.st));
-    // view chunks of ~128 MB, double-buffered
-    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(nangles, (128u << 20) / (npix * sizeof(float))));
+    if (int rc = S->get(0, nvox * sizeof(float), &dvol)) return rc;
+    TIGRE_CUDA(cudaMemcpyAsync(dvol, img, nvox * sizeof(float), cudaMemcpyHostToDevice, S->st));
+    // view chunks, double-buffered: D2H of chunk k (copy stream) overlaps the kernels of chunk k+1
+    const int chunk = (int)chunk_views(npix * sizeof(float), nangles);
     void* buf[2];
-    for (auto& b : buf)
-        if (int rc = h.alloc(&b, (size_t)chunk * npix * sizeof(float))) return rc;
-    int prev_a = -1, prev_n = 0, k = 0;
+    for (int i = 0; i < 2; ++i)
+        if (int rc = S->get(1 + i, (size_t)chunk * npix * sizeof(float), &buf[i])) return rc;
+    cudaEvent_t drained[2] = {S->ev[0], S->ev[1]}, computed[2] = {S->ev[2], S->ev[3]};
+    int k = 0;
     for (int a = 0; a < nangles; a += chunk, ++k) {
-        const int cnt = std::min(chunk, nangles - a);
-        // the copy stream must have drained this buffer (chunk k-2) before it is rewritten
-        TIGRE_CUDA(cudaStreamWaitEvent(h.st, h.ev[k % 2], 0));
-        if (int rc = tigre_ax(h.plan, dvol, TIGRE_F32, buf[k % 2], TIGRE_F32, projector, a, a + cnt, h.st)) return rc;
-        if (prev_a >= 0) {
-            const int pb = (k - 1) % 2;
-            for (int i = 0; i < prev_n; ++i)
-                TIGRE_CUDA(cudaMemcpyAsync(result[prev_a + i], (char*)buf[pb] + (size_t)i * npix * sizeof(float),
-                                           npix * sizeof(float), cudaMemcpyDeviceToHost, h.st2));
-            TIGRE_CUDA(cudaEventRecord(h.ev[pb], h.st2));
-        }
-        // copies of this chunk wait for its kernel
-        cudaEvent_t done;
-        TIGRE_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
-        cudaEventRecord(done, h.st);
-        cudaStreamWaitEvent(h.st2, done, 0);
-        cudaEventDestroy(done);
-        prev_a = a;
-        prev_n = cnt;
+        const int cnt = std::min(chunk, nangles - a), b = k % 2;
+        if (k >= 2) TIGRE_CUDA(cudaStreamWaitEvent(S->st, drained[b], 0));
+        if (int rc = tigre_ax(plan, dvol, TIGRE_F32, buf[b], TIGRE_F32, projector, a, a + cnt, S->st)) return rc;
+        TIGRE_CUDA(cudaEventRecord(computed[b], S->st));
+        TIGRE_CUDA(cudaStreamWaitEvent(S->st2, computed[b], 0));
+        for (int i = 0; i < cnt; ++i)
+            TIGRE_CUDA(cudaMemcpyAsync(result[a + i], (char*)buf[b] + (size_t)i * npix * sizeof(float),
+                                       npix * sizeof(float), cudaMemcpyDeviceToHost, S->st2));
+        TIGRE_CUDA(cudaEventRecord(drained[b], S->st2));
     }
-    if (prev_a >= 0) {
-        const int pb = (k - 1) % 2;
-        for (int i = 0; i < prev_n; ++i)
-            TIGRE_CUDA(cudaMemcpyAsync(result[prev_a + i], (char*)buf[pb] + (size_t)i * npix * sizeof(float),
-                                       npix * sizeof(float), cudaMemcpyDeviceToHost, h.st2));
-    }
-    TIGRE_CUDA(cudaStreamSynchronize(h.st2));
-    TIGRE_CUDA(cudaStreamSynchronize(h.st));
+    TIGRE_CUDA(cudaStreamSynchronize(S->st2));
+    TIGRE_CUDA(cudaStreamSynchronize(S->st));
     return TIGRE_SUCCESS;
 }
 
@@ -226,25 +299,74 @@ int host_backproject(const float* proj, const TigreGeometry* geo, float* result,
     int dev = 0;
     if (int rc = pick_device(ids, n, &dev)) return rc;
     DeviceGuard g(dev);
-    HostCall h;
-    if (int rc = tigre_plan_create(geo, angles, nangles, dev, &h.plan)) return rc;
-    const Dims& d = h.plan->d;
-    TIGRE_CUDA(cudaStreamCreateWithFlags(&h.st, cudaStreamNonBlocking));
-    const size_t nvox = (size_t)d.nX * d.nY * d.nZ, nproj = (size_t)nangles * d.nU * d.nV;
-    void *dvol = nullptr, *dproj = nullptr;
-    if (int rc = h.alloc(&dvol, nvox * sizeof(float))) return rc;
-    if (int rc = h.alloc(&dproj, nproj * sizeof(float))) return rc;
-    TIGRE_CUDA(cudaMemcpyAsync(dproj, proj, nproj * sizeof(float), cudaMemcpyHostToDevice, h.st));
-    if (int rc = tigre_atb(h.plan, dproj, TIGRE_F32, dvol, TIGRE_F32,
-                           matched ? TIGRE_BACKPROJ_MATCHED : TIGRE_BACKPROJ_FDK, 0, nangles, h.st))
-        return rc;
-    TIGRE_CUDA(cudaMemcpyAsync(result, dvol, nvox * sizeof(float), cudaMemcpyDeviceToHost, h.st));
-    TIGRE_CUDA(cudaStreamSynchronize(h.st));
-    if (tigre_plan_status(h.plan, 1) != 0) return fail(TIGRE_ERR_CUDA, "backprojection: a bounded wait expired");
+    DeviceState* S = state(dev);
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (int rc = S->init(dev)) return rc;
+    TigrePlan* plan = nullptr;
+    if (int rc = S->plan(geo, angles, nangles, dev, &plan)) return rc;
+    const Dims& d = plan->d;
+    const size_t nvox = (size_t)d.nX * d.nY * d.nZ, npix = (size_t)d.nU * d.nV;
+    void* dvol = nullptr;
+    if (int rc = S->get(0, nvox * sizeof(float), &dvol)) return rc;
+    // projection chunks, double-buffered: H2D of chunk k+1 (copy stream) overlaps the
+    // backprojection of chunk k, which accumulates into the volume
+    const int chunk = (int)chunk_views(npix * sizeof(float), nangles);
+    void* buf[2];
+    for (int i = 0; i < 2; ++i)
+        if (int rc = S->get(1 + i, (size_t)chunk * npix * sizeof(float), &buf[i])) return rc;
+    cudaEvent_t copied[2] = {S->ev[0], S->ev[1]}, consumed[2] = {S->ev[2], S->ev[3]};
+    const int bp = matched ? TIGRE_BACKPROJ_MATCHED : TIGRE_BACKPROJ_FDK;
+    int k = 0;
+    for (int a = 0; a < nangles; a += chunk, ++k) {
+        const int cnt = std::min(chunk, nangles - a), b = k % 2;
+        if (k >= 2) TIGRE_CUDA(cudaStreamWaitEvent(S->st2, consumed[b], 0));
+        TIGRE_CUDA(cudaMemcpyAsync(buf[b], proj + (size_t)a * npix, (size_t)cnt * npix * sizeof(float),
+                                   cudaMemcpyHostToDevice, S->st2));
+        TIGRE_CUDA(cudaEventRecord(copied[b], S->st2));
+        TIGRE_CUDA(cudaStreamWaitEvent(S->st, copied[b], 0));
+        if (int rc = tigre_atb_ex(plan, buf[b], TIGRE_F32, dvol, TIGRE_F32, bp, a, a + cnt, k > 0, S->st)) return rc;
+        TIGRE_CUDA(cudaEventRecord(consumed[b], S->st));
+    }
+    TIGRE_CUDA(cudaMemcpyAsync(result, dvol, nvox * sizeof(float), cudaMemcpyDeviceToHost, S->st));
+    TIGRE_CUDA(cudaStreamSynchronize(S->st));
+    TIGRE_CUDA(cudaStreamSynchronize(S->st2));
+    if (tigre_plan_status(plan, 1) != 0) return fail(TIGRE_ERR_CUDA, "backprojection: a bounded wait expired");
+    return TIGRE_SUCCESS;
+}
+
+int host_pocs_tv(const float* img, float* dst, float alpha, const long* image_size, int max_iter, const int* ids,
+                 int n) {
+    if (!img || !dst || !image_size) return fail(TIGRE_ERR_BAD_ASSERT, "null argument");
+    const long nx = image_size[0], ny = image_size[1], nz = image_size[2];
+    if (nx <= 0 || ny <= 0 || nz <= 0) return fail(TIGRE_ERR_BAD_ASSERT, "bad image size");
+    int dev = 0;
+    if (int rc = pick_device(ids, n, &dev)) return rc;
+    DeviceGuard g(dev);
+    DeviceState* S = state(dev);
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (int rc = S->init(dev)) return rc;
+    const size_t nvox = (size_t)nx * ny * nz;
+    void *dimg = nullptr, *dwork = nullptr;
+    if (int rc = S->get(0, nvox * sizeof(float), &dimg)) return rc;
+    if (int rc = S->get(1, nvox * sizeof(float), &dwork)) return rc;
+    TIGRE_CUDA(cudaMemcpyAsync(dimg, img, nvox * sizeof(float), cudaMemcpyHostToDevice, S->st));
+    if (int rc = tigre_tv_pocs(dimg, TIGRE_F32, nx, ny, nz, alpha, max_iter, (float*)dwork, S->st)) return rc;
+    TIGRE_CUDA(cudaMemcpyAsync(dst, dimg, nvox * sizeof(float), cudaMemcpyDeviceToHost, S->st));
+    TIGRE_CUDA(cudaStreamSynchronize(S->st));
     return TIGRE_SUCCESS;
 }
 
 }  // namespace
+
+extern "C" void tigre_release_cache(void) {
+    std::lock_guard<std::mutex> lk(g_states_mu);
+    for (size_t i = 0; i < g_states.size(); ++i) {
+        if (!g_states[i]) continue;
+        DeviceGuard g((int)i);
+        std::lock_guard<std::mutex> l2(g_states[i]->mu);
+        g_states[i]->release();
+    }
+}
 
 extern "C" {
 
@@ -270,23 +392,7 @@ int tigre_voxel_backprojection2(const float* proj, const TigreGeometry* geo, flo
 
 int tigre_pocs_tv(const float* img, float* dst, float alpha, const long* image_size, int max_iter, const int* ids,
                   int n) {
-    if (!img || !dst || !image_size) return fail(TIGRE_ERR_BAD_ASSERT, "null argument");
-    const long nx = image_size[0], ny = image_size[1], nz = image_size[2];
-    if (nx <= 0 || ny <= 0 || nz <= 0) return fail(TIGRE_ERR_BAD_ASSERT, "bad image size");
-    int dev = 0;
-    if (int rc = pick_device(ids, n, &dev)) return rc;
-    DeviceGuard g(dev);
-    HostCall h;
-    TIGRE_CUDA(cudaStreamCreateWithFlags(&h.st, cudaStreamNonBlocking));
-    const size_t nvox = (size_t)nx * ny * nz;
-    void *dimg = nullptr, *dwork = nullptr;
-    if (int rc = h.alloc(&dimg, nvox * sizeof(float))) return rc;
-    if (int rc = h.alloc(&dwork, nvox * sizeof(float))) return rc;
-    TIGRE_CUDA(cudaMemcpyAsync(dimg, img, nvox * sizeof(float), cudaMemcpyHostToDevice, h.st));
-    if (int rc = tigre_tv_pocs(dimg, TIGRE_F32, nx, ny, nz, alpha, max_iter, (float*)dwork, h.st)) return rc;
-    TIGRE_CUDA(cudaMemcpyAsync(dst, dimg, nvox * sizeof(float), cudaMemcpyDeviceToHost, h.st));
-    TIGRE_CUDA(cudaStreamSynchronize(h.st));
-    return TIGRE_SUCCESS;
+    return host_pocs_tv(img, dst, alpha, image_size, max_iter, ids, n);
 }
 
 int tigre_siddon_ray_projection_parallel(const float*, const TigreGeometry*, float* const*, const float*, int,

@@ -40,6 +40,7 @@ struct BPArgs {
     float sVX, sVY, sVZ, dVX, dVY, dVZ;
     float sDU, sDV, dDU, dDV;
     float scale;
+    int accumulate;       // add into the existing volume instead of overwriting it
 };
 
 constexpr int BX = 32, BY = 8, CHUNK = 32;
@@ -173,7 +174,11 @@ __global__ void __launch_bounds__(BX* BY) bp_kernel(BPArgs p) {
 #pragma unroll
     for (int k = 0; k < VZ; ++k) {
         const int z = z0 + k;
-        if (z < p.nZ) V[((size_t)z * p.nY + y) * p.nX + x] = from_f32<TV>(acc[k] * p.scale);
+        if (z < p.nZ) {
+            const size_t i = ((size_t)z * p.nY + y) * p.nX + x;
+            const float o = p.accumulate ? to_f32<TV>(V[i]) : 0.f;
+            V[i] = from_f32<TV>(fmaf(acc[k], p.scale, o));
+        }
     }
 }
 
@@ -195,7 +200,7 @@ void launch_typed(const BPArgs& a, bool matched, bool axial, cudaStream_t st) {
 }  // namespace
 
 int launch_backproject(TigrePlan* P, const void* proj_pad, int pdt, void* vol, int vdt, int matched, int a0, int a1,
-                       cudaStream_t st) {
+                       int accumulate, cudaStream_t st) {
     static_assert(sizeof(FrameBP) % 4 == 0, "frame must be word-sized");
     BPArgs a{};
     a.proj = proj_pad; a.vol = vol; a.frames = P->d_bp; a.a0 = a0; a.na = a1 - a0;
@@ -204,6 +209,7 @@ int launch_backproject(TigrePlan* P, const void* proj_pad, int pdt, void* vol, i
     a.dVX = (float)P->d.dVX; a.dVY = (float)P->d.dVY; a.dVZ = (float)P->d.dVZ;
     a.sDU = (float)P->d.sDU; a.sDV = (float)P->d.sDV; a.dDU = (float)P->d.dDU; a.dDV = (float)P->d.dDV;
     a.scale = matched ? (float)(P->d.dVX * P->d.dVY * P->d.dVZ / (P->d.dDU * P->d.dDV)) : 1.f;
+    a.accumulate = accumulate;
     const bool ax = P->axial;
     if (pdt == TIGRE_F32 && vdt == TIGRE_F32) launch_typed<float, float>(a, matched, ax, st);
     else if (pdt == TIGRE_BF16 && vdt == TIGRE_BF16) launch_typed<__nv_bfloat16, __nv_bfloat16>(a, matched, ax, st);

@@ -46,6 +46,7 @@ struct BPKArgs {
     int BU, BV;           // patch box
     float dVZ;
     float scale;
+    int accumulate;       // add into the existing volume instead of overwriting it
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -258,14 +259,31 @@ __global__ void __launch_bounds__(TXY* TXY) bp_tma_kernel(const __grid_constant_
                         dvz2 = f2(p.dVZ); rz2 = f2(fmaf((float)z0, p.dVZ, F.rv0z)); dsd2 = f2(F.dsd);
                     }
                     const float2 w2 = f2(wcol);
+                    // rows stay inside the patch for the whole column -> no per-voxel clamps
+                    const float pvlast = fmaf((float)(VZ - 1), vstep, pv0);
+                    const bool inside = fminf(pv0, pvlast) >= 0.f && fmaxf(pv0, pvlast) <= pvmax;
+                    // Newton-Raphson seeds for the matched weight (refined per slice pair below)
+                    float2 ys = f2(0.f), rs = f2(0.f);
+                    if (MATCHED) {
+                        const float vt = vt0, dz = fmaf(vt, F.ddv, F.dzc), L2 = fmaf(dz, dz, cu2);
+                        const float rvz = fmaf((float)z0, p.dVZ, F.rv0z), lsq = fmaf(rvz, rvz, cxy);
+                        ys = f2(rsqrtf(L2));
+                        rs = f2(__fdividef(1.f, F.dsd * lsq));
+                    }
 #pragma unroll
                     for (int k = 0; k < VZ; k += 2) {
                         const float2 kk = f2((float)k, (float)(k + 1));
                         float2 pv = __ffma2_rn(kk, vstep2, pv02);
-                        pv.x = fminf(fmaxf(pv.x, 0.f), pvmax);
-                        pv.y = fminf(fmaxf(pv.y, 0.f), pvmax);
-                        const int ia = (int)pv.x, ib = (int)pv.y;
-                        const float2 fv = __fadd2_rn(pv, f2(-(float)ia, -(float)ib));
+                        if (!inside) {
+                            pv.x = fminf(fmaxf(pv.x, 0.f), pvmax);
+                            pv.y = fminf(fmaxf(pv.y, 0.f), pvmax);
+                        }
+                        // floor / fraction with packed arithmetic: pv >= 0 here, and at 1.5*2^23
+                        // the float spacing is 1, so a round-toward-zero add of 1.5*2^23 leaves
+                        // floor(pv) in the low mantissa bits; subtracting it back is exact
+                        const float2 t = __fadd2_rz(pv, f2(12582912.0f));
+                        const int ia = __float_as_int(t.x) - 0x4B400000, ib = __float_as_int(t.y) - 0x4B400000;
+                        const float2 fv = __fadd2_rn(pv, neg2(__fadd2_rn(t, f2(-12582912.0f))));
                         const uint32_t aa = colb + (uint32_t)ia * rowb, ab = colb + (uint32_t)ib * rowb;
                         const float2 r0 = f2(lds<TP>(aa), lds<TP>(ab)), r0r = f2(lds<TP>(aa + ES), lds<TP>(ab + ES));
                         const float2 r1 = f2(lds<TP>(aa + rowb), lds<TP>(ab + rowb));
@@ -273,22 +291,26 @@ __global__ void __launch_bounds__(TXY* TXY) bp_tma_kernel(const __grid_constant_
                         const float2 smp = lerp2(lerp2(r0, r0r, fu2), lerp2(r1, r1r, fu2), fv);
                         float2 w = w2;
                         if (MATCHED) {
+                            // w = L^3 / (DSD lsq); 1/sqrt(L^2) and 1/(DSD lsq) change by ~1e-4 relative per
+                            // slice, so one Newton-Raphson step from the previous pair's values
+                            // (y <- y (3 - x y^2)/2 ;  r <- r (2 - d r)) is accurate to ~1e-8
                             const float2 vtex = __ffma2_rn(kk, vstep2, vt02);
                             const float2 dz = __ffma2_rn(vtex, ddv2, dzc2);
                             const float2 L2 = __ffma2_rn(dz, dz, cu22);
                             const float2 rvz = __ffma2_rn(kk, dvz2, rz2);
-                            const float2 lsq = __ffma2_rn(rvz, rvz, cxy2);
-                            const float2 rs = f2(rsqrtf(L2.x), rsqrtf(L2.y));
-                            const float2 L3 = __fmul2_rn(L2, __fmul2_rn(L2, rs));
-                            const float2 den = __fmul2_rn(lsq, dsd2);
-                            w = __fmul2_rn(L3, f2(__fdividef(1.f, den.x), __fdividef(1.f, den.y)));
+                            const float2 den = __fmul2_rn(__ffma2_rn(rvz, rvz, cxy2), dsd2);
+                            const float2 hl = __fmul2_rn(L2, f2(-0.5f));
+                            ys = __fmul2_rn(ys, __ffma2_rn(hl, __fmul2_rn(ys, ys), f2(1.5f)));
+                            rs = __fmul2_rn(rs, __ffma2_rn(neg2(den), rs, f2(2.0f)));
+                            w = __fmul2_rn(__fmul2_rn(L2, L2), __fmul2_rn(ys, rs));
                         }
                         const float2 acc2 = __ffma2_rn(smp, w, f2(acc[k], acc[k + 1]));
                         acc[k] = acc2.x;
                         acc[k + 1] = acc2.y;
                     }
                 } else {
-#pragma unroll 1
+                    // unrolled: a runtime index into acc[] would move it to local memory
+#pragma unroll
                     for (int k = 0; k < VZ; ++k) {
                         const float vtex = fmaf((float)k, vstep, vt0);
                         const float smp = global_sample<TP>(p, Pg + (long)la * p.pitch * p.nV, u - 0.5f, vtex - 0.5f);
@@ -347,7 +369,11 @@ __global__ void __launch_bounds__(TXY* TXY) bp_tma_kernel(const __grid_constant_
 #pragma unroll
     for (int k = 0; k < VZ; ++k) {
         const int z = z0 + k;
-        if (z < p.nZ) V[((size_t)z * p.nY + y) * p.nX + x] = from_f32<TV>(acc[k] * p.scale);
+        if (z < p.nZ) {
+            const size_t i = ((size_t)z * p.nY + y) * p.nX + x;
+            const float o = p.accumulate ? to_f32<TV>(V[i]) : 0.f;
+            V[i] = from_f32<TV>(fmaf(acc[k], p.scale, o));
+        }
     }
 }
 
@@ -386,7 +412,7 @@ bool bp_tma_supported(const TigrePlan* P, int pdt) {
 }
 
 int launch_backproject_tma(TigrePlan* P, const void* proj, int pitch, int pdt, void* vol, int vdt, int matched,
-                           int a0, int a1, cudaStream_t st) {
+                           int a0, int a1, int accumulate, cudaStream_t st) {
     auto enc = encode_fn();
     if (!enc) return fail(TIGRE_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
     const int na = a1 - a0;
@@ -413,6 +439,7 @@ int launch_backproject_tma(TigrePlan* P, const void* proj, int pitch, int pdt, v
     a.BV = P->bp_box_v;
     a.dVZ = (float)P->d.dVZ;
     a.scale = matched ? (float)(P->d.dVX * P->d.dVY * P->d.dVZ / (P->d.dDU * P->d.dDV)) : 1.f;
+    a.accumulate = accumulate;
     const bool ax = P->axial;
     if (pdt == TIGRE_F32 && vdt == TIGRE_F32) return launch_typed<float, float>(tm, a, matched, ax, st);
     if (pdt == TIGRE_BF16 && vdt == TIGRE_BF16) return launch_typed<__nv_bfloat16, __nv_bfloat16>(tm, a, matched, ax, st);

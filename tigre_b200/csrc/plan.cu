@@ -147,6 +147,17 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
         fs.layout = std::fabs(Pu.y) >= std::fabs(Pu.x) ? 1 : 0;
         fs.pad_ = 0;
         if (Pv.x != 0.0 || Pv.y != 0.0) columns = false;
+        // steepest ray of this view: bounds the z crossings per xy cell.  |rz| is largest at
+        // the first or last row; over u the ratio is sampled at 65 columns (and the threshold
+        // used against it keeps a factor-2 margin)
+        for (int cu = 0; cu <= 64; ++cu)
+            for (int cv = 0; cv < 2; ++cv) {
+                const double uu = (d.nU - 1) * (cu / 64.0), vv = cv ? d.nV - 1 : 0;
+                const double rx = P.x + uu * Pu.x + vv * Pv.x - S.x, ry = P.y + uu * Pu.y + vv * Pv.y - S.y;
+                const double rz = P.z + uu * Pu.z + vv * Pv.z - S.z;
+                const double dom = std::max(std::fabs(rx), std::fabs(ry));
+                plan->column_slope_max = std::max(plan->column_slope_max, dom > 0 ? std::fabs(rz) / dom : 1e30);
+            }
 
         // ---- interpolated frame: voxel centres at integers (computeDeltas) ----
         FrameInterp& fi = plan->h_interp[i];

@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(256) siddon_count_kernel(SiddonArgs p) {
 // leaves the volume through its top or bottom reads zeros.  Grid order
 // (column groups fastest, then views, then row tiles) keeps the z-slab of the
 // current row tile L2-resident while every view is processed.
-template <typename TV, typename TP, int R>
+template <typename TV, typename TP, int R, bool SINGLE>
 __global__ void __launch_bounds__(128, 6) siddon_columns_kernel(SiddonArgs p) {
     const int lane = threadIdx.x & 31;
     const int u = blockIdx.x * 4 + (threadIdx.x >> 5);
@@ -312,10 +312,10 @@ __global__ void __launch_bounds__(128, 6) siddon_columns_kernel(SiddonArgs p) {
                 iz[r] = izn;
                 kz[r] += 1.f;
                 tz[r] = fmaf(kz[r], dtz[r], tz0[r]);
-                again |= tz[r] < b;
+                if (!SINGLE) again |= tz[r] < b;
             }
         }
-        if (__any_sync(0xffffffffu, again)) {
+        if (!SINGLE && __any_sync(0xffffffffu, again)) {
             // steep rays: further crossings inside the same cell (warp-uniform, rare)
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -396,11 +396,17 @@ int launch_siddon(TigrePlan* P, const void* vol_x, const void* vol_y, int vdt, v
     return TIGRE_SUCCESS;
 }
 
+template <typename TV, typename TP, bool SINGLE>
+static void launch_columns_r(const SiddonArgs& a, int rows_per_thread, dim3 grid, cudaStream_t st) {
+    if (rows_per_thread == 4) siddon_columns_kernel<TV, TP, 4, SINGLE><<<grid, 128, 0, st>>>(a);
+    else if (rows_per_thread == 2) siddon_columns_kernel<TV, TP, 2, SINGLE><<<grid, 128, 0, st>>>(a);
+    else siddon_columns_kernel<TV, TP, 1, SINGLE><<<grid, 128, 0, st>>>(a);
+}
+
 template <typename TV, typename TP>
-static void launch_columns_typed(const SiddonArgs& a, int rows_per_thread, dim3 grid, cudaStream_t st) {
-    if (rows_per_thread == 4) siddon_columns_kernel<TV, TP, 4><<<grid, 128, 0, st>>>(a);
-    else if (rows_per_thread == 2) siddon_columns_kernel<TV, TP, 2><<<grid, 128, 0, st>>>(a);
-    else siddon_columns_kernel<TV, TP, 1><<<grid, 128, 0, st>>>(a);
+static void launch_columns_typed(const SiddonArgs& a, int rows_per_thread, bool single, dim3 grid, cudaStream_t st) {
+    if (single) launch_columns_r<TV, TP, true>(a, rows_per_thread, grid, st);
+    else launch_columns_r<TV, TP, false>(a, rows_per_thread, grid, st);
 }
 
 int launch_siddon_columns(TigrePlan* P, const void* vol_z, int vdt, void* proj, int pdt, int a0, int a1,
@@ -410,19 +416,21 @@ int launch_siddon_columns(TigrePlan* P, const void* vol_z, int vdt, void* proj, 
     a.proj = proj;
     const int nv = P->d.nV;
     const int R = nv >= 512 ? 4 : (nv >= 128 ? 2 : 1);
+    // z advance per xy segment <= slope: below 1 a segment crosses at most one z plane
+    const bool single = P->column_slope_max < 0.5;
     const int na = a1 - a0;
     for (int c = 0; c < na; c += 65535) {
         SiddonArgs ac = a;
         ac.a0 = a0 + c;
         ac.proj = (char*)proj + (size_t)c * P->d.nU * P->d.nV * dtype_size(pdt);
         dim3 grid((P->d.nU + 3) / 4, std::min(65535, na - c), (nv + 32 * R - 1) / (32 * R));
-        if (vdt == TIGRE_F32 && pdt == TIGRE_F32) launch_columns_typed<float, float>(ac, R, grid, st);
-        else if (vdt == TIGRE_BF16 && pdt == TIGRE_BF16) launch_columns_typed<__nv_bfloat16, __nv_bfloat16>(ac, R, grid, st);
-        else if (vdt == TIGRE_F16 && pdt == TIGRE_F16) launch_columns_typed<__half, __half>(ac, R, grid, st);
-        else if (vdt == TIGRE_BF16 && pdt == TIGRE_F32) launch_columns_typed<__nv_bfloat16, float>(ac, R, grid, st);
-        else if (vdt == TIGRE_F16 && pdt == TIGRE_F32) launch_columns_typed<__half, float>(ac, R, grid, st);
-        else if (vdt == TIGRE_F32 && pdt == TIGRE_BF16) launch_columns_typed<float, __nv_bfloat16>(ac, R, grid, st);
-        else if (vdt == TIGRE_F32 && pdt == TIGRE_F16) launch_columns_typed<float, __half>(ac, R, grid, st);
+        if (vdt == TIGRE_F32 && pdt == TIGRE_F32) launch_columns_typed<float, float>(ac, R, single, grid, st);
+        else if (vdt == TIGRE_BF16 && pdt == TIGRE_BF16) launch_columns_typed<__nv_bfloat16, __nv_bfloat16>(ac, R, single, grid, st);
+        else if (vdt == TIGRE_F16 && pdt == TIGRE_F16) launch_columns_typed<__half, __half>(ac, R, single, grid, st);
+        else if (vdt == TIGRE_BF16 && pdt == TIGRE_F32) launch_columns_typed<__nv_bfloat16, float>(ac, R, single, grid, st);
+        else if (vdt == TIGRE_F16 && pdt == TIGRE_F32) launch_columns_typed<__half, float>(ac, R, single, grid, st);
+        else if (vdt == TIGRE_F32 && pdt == TIGRE_BF16) launch_columns_typed<float, __nv_bfloat16>(ac, R, single, grid, st);
+        else if (vdt == TIGRE_F32 && pdt == TIGRE_F16) launch_columns_typed<float, __half>(ac, R, single, grid, st);
         else return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype pair for Siddon");
         TIGRE_CUDA(cudaGetLastError());
     }

@@ -106,6 +106,7 @@ struct TigrePlan {
     tigre::FrameBP* d_bp = nullptr;
     bool axial = false;          // every BP frame has dz.x == dz.y == 0 (u constant along z)
     bool columns = false;        // every Siddon frame has dv.x == dv.y == 0 (detector v parallel to z)
+    double column_slope_max = 0; // max over rays of |rz| / max(|rx|, |ry|): z change per xy cell
     std::vector<tigre::FrameBPK> h_bpk;
     tigre::FrameBPK* d_bpk = nullptr;
     int bp_box_u = 0, bp_box_v = 0;   // TMA patch box of the staged backprojector (0: not usable)
@@ -134,11 +135,11 @@ int launch_siddon_columns(TigrePlan* p, const void* vol_z, int vdt, void* proj, 
 int launch_interp(TigrePlan* p, const void* vol_x, const void* vol_y, int vdt, void* proj, int pdt, int a0, int a1,
                   cudaStream_t st);
 int launch_backproject(TigrePlan* p, const void* proj_pad, int pdt, void* vol, int vdt, int matched, int a0, int a1,
-                       cudaStream_t st);
+                       int accumulate, cudaStream_t st);
 
 bool bp_tma_supported(const TigrePlan* p, int pdt);
 int launch_backproject_tma(TigrePlan* p, const void* proj, int pitch, int pdt, void* vol, int vdt, int matched,
-                           int a0, int a1, cudaStream_t st);
+                           int a0, int a1, int accumulate, cudaStream_t st);
 int launch_repitch_projections(const void* src, int dtype, void* dst, int nA, int nV, int nU, int pitch,
                                cudaStream_t st);
 

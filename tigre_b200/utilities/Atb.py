@@ -31,8 +31,8 @@ def Atb(projections, geo, angles, backprojection_type="FDK", **kwargs):  # noqa:
         return projectors.atb(projections.contiguous(), plan, _backprojector_name(backprojection_type))
     if projections.dtype != np.float32:
         raise TypeError("Input data should be float32, not " + str(projections.dtype))
-    if not np.isreal(projections).all():
-        raise ValueError("Complex types not compatible for back projection.")
+    # np.isreal(projections).all() (Atb.py:12-13) is always true for float32 and costs a full
+    # pass over the projections: omitted
     geox = N.checked_geometry(geo, angles)
     want = (geox.angles.shape[0], int(geox.nDetector[0]), int(geox.nDetector[1]))
     if projections.shape != want:
@@ -45,7 +45,7 @@ def _atb_host(projections, geox, backprojection_type, mode, devices):
     btype = _backprojector_name(backprojection_type)
     angles = np.ascontiguousarray(np.asarray(geox.angles, dtype=np.float32).reshape(-1, 3))
     n = angles.shape[0]
-    out = np.empty(tuple(int(v) for v in geox.nVoxel), dtype=np.float32)
+    out = N.host_empty(tuple(int(v) for v in geox.nVoxel))
     cg = N.CGeometry(geox, n)
     ids = (C.c_int * len(devices))(*devices)
     proj = np.ascontiguousarray(projections)

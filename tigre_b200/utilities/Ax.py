@@ -28,8 +28,8 @@ def Ax(img, geo, angles, projection_type="Siddon", **kwargs):  # noqa: N802
         return projectors.ax(img.contiguous(), plan, _projector_name(projection_type))
     if img.dtype != np.float32:
         raise TypeError("Input data should be float32, not " + str(img.dtype))
-    if not np.isreal(img).all():
-        raise ValueError("Complex types not compatible for projection.")
+    # the reference's np.isreal(img).all() check follows here (Ax.py:32-33); after the float32
+    # test it is always true and costs a full pass over the volume, so it is omitted
     if any(np.asarray(img.shape) != np.asarray(geo.nVoxel)):
         raise ValueError("Input data should be of shape geo.nVoxel: " + str(geo.nVoxel) + " not:" + str(img.shape))
     geox = N.checked_geometry(geo, angles)
@@ -51,7 +51,7 @@ def _ax_host(img, geox, projection_type, mode, devices):
     angles = np.ascontiguousarray(np.asarray(geox.angles, dtype=np.float32).reshape(-1, 3))
     n = angles.shape[0]
     nv, nu = int(geox.nDetector[0]), int(geox.nDetector[1])
-    out = np.empty((n, nv, nu), dtype=np.float32)
+    out = N.host_empty((n, nv, nu))
     rows = (C.c_void_p * n)(*[out.ctypes.data + i * nv * nu * 4 for i in range(n)])
     cg = N.CGeometry(geox, n)
     ids = (C.c_int * len(devices))(*devices)
