@@ -171,6 +171,14 @@ int tigre_siddon_count_segments(TigrePlan* plan, int angle_begin, int angle_end,
  * d_work: caller scratch of nx*ny*nz floats (same dtype as d_img is not required: FP32). */
 int tigre_tv_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha, int max_iter, float* d_work,
                   void* stream);
+/* As tigre_tv_pocs, but allocates no device memory (no counterpart in the reference).
+ * The per-iteration norm sums live in a fixed 32 KiB device array of the library, so
+ * max_iter <= 4096 (larger values return TIGRE_ERR_BAD_ASSERT).  All calls on a device
+ * share that array: calls that overlap in time on one device race and must be
+ * serialised by the caller.  The first call on each device looks up the array's
+ * address with that device current; make it before any stream capture. */
+int tigre_tv_pocs_noalloc(void* d_img, int dtype, long nx, long ny, long nz, float alpha, int max_iter,
+                          float* d_work, void* stream);
 /* TV gradient (GD_TV.cu:117-143, single-device boundary rule) into d_grad (FP32). */
 int tigre_tv_gradient(const void* d_img, int dtype, float* d_grad, long nx, long ny, long nz, void* stream);
 /* TV value sum_i |grad f_i| consistent with tigre_tv_gradient; added into *d_out (FP64). */

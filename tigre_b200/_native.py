@@ -84,6 +84,8 @@ _SIGS = {
     "tigre_siddon_count_segments": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "tigre_tv_pocs": (C.c_int, [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_int, C.c_void_p,
                                 C.c_void_p]),
+    "tigre_tv_pocs_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_int,
+                                        C.c_void_p, C.c_void_p]),
     "tigre_tv_gradient": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_long, C.c_long, C.c_long, C.c_void_p]),
     "tigre_tv_value": (C.c_int, [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_long, C.c_void_p, C.c_void_p]),
     "tigre_sumsq": (C.c_int, [C.c_void_p, C.c_int, C.c_long, C.c_void_p, C.c_void_p]),

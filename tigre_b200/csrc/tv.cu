@@ -17,6 +17,8 @@
 // and the terms of neighbours beyond the last x / y index vanish.
 
 #include <cmath>
+#include <mutex>
+#include <string>
 
 #include "tigre_internal.h"
 
@@ -207,3 +209,72 @@ int tigre_tv_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha
 }
 
 }  // extern "C"
+
+// POCS-TV that allocates nothing.
+//
+// Who needs it: a caller whose process has handed all free device memory to another
+// allocator (a framework's caching pool, a service run under a fixed memory cap) gets
+// no memory from cudaMallocAsync, and a caller inside a fixed-latency loop must not
+// enter the allocator at all, since allocation can block on locks or on the device.
+// For those callers the only scratch of tigre_tv_pocs besides d_work -- one FP64 norm
+// sum per iteration -- lives here in a fixed array of this module's device memory.
+//
+// Limits and sharing: the array holds kTvPocsStaticMaxIter sums, so max_iter above it
+// is rejected.  Every call on a device uses the same array, and the first max_iter
+// entries must be zero when a call's first kernel runs: each call clears them on its
+// stream before use.  Calls that overlap in time on one device (other streams, other
+// host threads) therefore race on the sums and must be serialised by the caller.
+// The first call on each device looks up the array's address with that device
+// current and caches it; make that first call before any stream capture.
+constexpr int kTvPocsStaticMaxIter = 4096;   // 32 KiB
+static __device__ __align__(256) double g_tv_pocs_sums[kTvPocsStaticMaxIter];
+
+namespace {
+constexpr int kMaxDevices = 256;
+std::mutex g_tv_pocs_sums_mu;
+double* g_tv_pocs_sums_addr[kMaxDevices] = {};
+
+// Address of g_tv_pocs_sums on the current device (looked up once per device).
+int tv_pocs_static_sums(double** out) {
+    int dev = 0;
+    TIGRE_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(TIGRE_ERR_BAD_ASSERT, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_tv_pocs_sums_mu);
+    if (!g_tv_pocs_sums_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_tv_pocs_sums);
+        if (e != cudaSuccess || !p) return cuda_fail(e, "cudaGetSymbolAddress(g_tv_pocs_sums)");
+        g_tv_pocs_sums_addr[dev] = (double*)p;
+    }
+    *out = g_tv_pocs_sums_addr[dev];
+    return TIGRE_SUCCESS;
+}
+}  // namespace
+
+extern "C" int tigre_tv_pocs_noalloc(void* d_img, int dtype, long nx, long ny, long nz, float alpha, int max_iter,
+                                     float* d_work, void* stream) {
+    if (dtype != TIGRE_F32) return fail(TIGRE_ERR_BAD_ASSERT, "TV kernels take float32 volumes");
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !d_img || !d_work || max_iter < 0)
+        return fail(TIGRE_ERR_BAD_ASSERT, "bad TV arguments");
+    if ((double)nx * ny * nz >= 2147483647.0) return fail(TIGRE_ERR_BAD_ASSERT, "volume too large");
+    if (max_iter > kTvPocsStaticMaxIter)
+        return fail(TIGRE_ERR_BAD_ASSERT, "tigre_tv_pocs_noalloc: max_iter " + std::to_string(max_iter) +
+                                              " exceeds its fixed scratch of " +
+                                              std::to_string(kTvPocsStaticMaxIter) + " iterations");
+    double* sums = nullptr;
+    if (int rc = tv_pocs_static_sums(&sums)) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    TVDims d{(int)nx, (int)ny, (int)nz};
+    const size_t n = (size_t)nx * ny * nz;
+    if (max_iter > 0) TIGRE_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)max_iter, st));
+    float* cur = (float*)d_img;
+    float* nxt = d_work;
+    for (int it = 0; it < max_iter; ++it) {
+        tv_norm_kernel<<<grid_for(n), 256, 0, st>>>(cur, d, sums + it);
+        tv_update_kernel<<<grid_for(n), 256, 0, st>>>(cur, nxt, d, sums + it, alpha);
+        std::swap(cur, nxt);
+    }
+    if (cur != (float*)d_img) TIGRE_CUDA(cudaMemcpyAsync(d_img, cur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    TIGRE_CUDA(cudaGetLastError());
+    return TIGRE_SUCCESS;
+}
