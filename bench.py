@@ -193,6 +193,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ops", action="store_true", help="skip the per-kind kernel timings")
     ap.add_argument("--size", type=int, default=512, choices=[512, 256])
     ap.add_argument("--views", type=int, default=0)
     args = ap.parse_args()
@@ -230,6 +231,7 @@ def main():
     clk.start()
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     torch.cuda.synchronize()
+    launches0 = N.lib().tigre_launch_count()
     for k in range(args.steps):
         ev[k][0].record()
         P.ax(vol, plan, "Siddon", out=proj)
@@ -237,6 +239,7 @@ def main():
         P.atb(proj, plan, "matched", out=bp)
         ev[k][2].record()
     torch.cuda.synchronize()
+    launches = N.lib().tigre_launch_count() - launches0
     if dist:
         dist.barrier()
     clocks = clk.stop()
@@ -257,16 +260,20 @@ def main():
     atb_launch = t_atb / args.steps
     if ax_launch >= atb_launch:
         alg = nseg * 4 + rays * 4           # one voxel gather per Siddon segment + one output write per ray
-        roof = {"kernel": "siddon_kernel<float,float>", "bound": "hbm", "achieved": alg / ax_launch / 1e9,
-                "alg_bytes_per_launch": alg}
+        roof = {"kernel": "siddon_cells_kernel<float,float,4>", "bound": "hbm",
+                "achieved": alg / ax_launch / 1e9, "alg_bytes_per_launch": alg,
+                "traffic": _scaled_traffic("siddon", NA)}
     else:
         alg = upd * 4 * 4 + math.prod(NVOX) * 4   # 4 bilinear taps per update + one volume write
-        roof = {"kernel": "bp_kernel<matched>", "bound": "hbm", "achieved": alg / atb_launch / 1e9,
-                "alg_bytes_per_launch": alg}
-    roof.update({"peak": peak, "unit": "GB/s", "frac": roof["achieved"] / peak, "peak_source": peak_kind,
-                 "traffic": None})
+        roof = {"kernel": "bp_tma_kernel<float,float,true,true>", "bound": "hbm",
+                "achieved": alg / atb_launch / 1e9, "alg_bytes_per_launch": alg,
+                "traffic": _scaled_traffic("bp", NA)}
+    roof.update({"peak": peak, "unit": "GB/s", "frac": roof["achieved"] / peak, "peak_source": peak_kind})
     for k in ("achieved", "frac"):
         roof[k] = round(roof[k], 4)
+    ops = None
+    if not args.no_ops:
+        ops = time_ops(P, plan, vol, proj)
     e2e = None
     if not args.no_e2e and rank == 0:
         e2e = measure_e2e(vol, geo, ang, min(args.steps, 3))
@@ -278,16 +285,19 @@ def main():
             "warmup": max(3, args.warmup), "ms_per_step": round(1e3 * t_tot / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded random ellipsoids)",
-            "config": {"workload": WORKLOAD, "step": "Siddon Ax of 720 views + matched Atb",
-                       "l2": "inputs larger than L2 (volume 512 MiB, projections 2.1 GiB)",
+            "config": {"workload": WORKLOAD, "step": "Siddon Ax of %d views + matched Atb of them" % NA,
+                       "l2": "inputs larger than L2: no flush (volume %.0f MiB, projections %.2f GiB)" % (
+                           math.prod(NVOX) * 4 / 2 ** 20, NA * NU * NV * 4 / 2 ** 30),
                        "parallelism": "replicas" if world > 1 else "single"},
             "atb": {"value": round(atb_value, 4), "unit": "Gvox-upd/s", "ms_per_launch": round(1e3 * atb_launch, 3)},
             "ax_ms_per_launch": round(1e3 * ax_launch, 3),
             "siddon_segments": nseg,
             "roofline": roof,
-            "gpu_launches": 4 * args.steps,
+            "gpu_launches": int(launches),
             "clocks": clocks,
         }
+        if ops:
+            line["ops"] = ops
         if e2e:
             line["e2e"] = e2e
         if not args.no_cpu:
@@ -298,6 +308,51 @@ def main():
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
+
+
+# DRAM bytes per launch per view, from ncu captures of the 512^3 workload at 36 views
+# (dram__bytes_read.sum + dram__bytes_write.sum; profiles/siddon_columns_512cube_36views.txt and
+# profiles/bp_tma_matched_512cube_36views.txt), scaled to the timed launch by its view count.
+# Traffic grows with the views processed: the volume is re-read per view group, the projections
+# are read or written once.
+TRAFFIC_PER_VIEW = {"siddon": None, "bp": None}
+
+
+def _scaled_traffic(kind, views):
+    per_view = TRAFFIC_PER_VIEW.get(kind) if NVOX == (512, 512, 512) and NU == 1024 else None
+    return None if per_view is None else int(per_view * views)
+
+
+def time_ops(P, plan, vol, proj, reps=3):
+    """Kernel-only time per launch of the other projector kinds and of BF16 storage
+    (same workload, CUDA events, one untimed launch first)."""
+    import torch
+    vol16, proj16 = vol.to(torch.bfloat16), proj.to(torch.bfloat16)
+    p_out, v_out = torch.empty_like(proj), torch.empty_like(vol)
+    p16_out, v16_out = torch.empty_like(proj16), torch.empty_like(vol16)
+    rays, upd = NA * NU * NV, NA * math.prod(NVOX)
+    cases = {
+        "ax_interpolated_f32": (lambda: P.ax(vol, plan, "interpolated", out=p_out), rays, "GRays/s"),
+        "atb_fdk_f32": (lambda: P.atb(proj, plan, "FDK", out=v_out), upd, "Gvox-upd/s"),
+        "ax_siddon_bf16": (lambda: P.ax(vol16, plan, "Siddon", out=p16_out), rays, "GRays/s"),
+        "ax_interpolated_bf16": (lambda: P.ax(vol16, plan, "interpolated", out=p16_out), rays, "GRays/s"),
+        "atb_matched_bf16": (lambda: P.atb(proj16, plan, "matched", out=v16_out), upd, "Gvox-upd/s"),
+        "atb_fdk_bf16": (lambda: P.atb(proj16, plan, "FDK", out=v16_out), upd, "Gvox-upd/s"),
+    }
+    out = {}
+    for name, (fn, units, unit) in cases.items():
+        fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        dt = e0.elapsed_time(e1) / 1e3 / reps
+        out[name] = {"value": round(units / dt / 1e9, 4), "unit": unit, "ms_per_launch": round(1e3 * dt, 3)}
+    del vol16, proj16, p_out, v_out, p16_out, v16_out
+    return out
 
 
 def measure_e2e(vol, geo, ang, steps):

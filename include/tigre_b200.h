@@ -77,6 +77,8 @@ typedef struct TigreGeometry {
 const char* tigre_last_error(void);
 /* Library version (major*100 + minor). */
 int tigre_version(void);
+/* Number of kernels this library has launched in this process, on all devices. */
+unsigned long long tigre_launch_count(void);
 
 /* ---------------------------------------------------------------------------
  * 1. Drop-in host-pointer entry points.

@@ -272,3 +272,31 @@ print('ok')
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env,
                        cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))), timeout=600)
     assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
+
+
+def test_column_kernel_without_cell_intervals():
+    """TIGRE_B200_NO_CELLS=1 keeps the stepped column kernel (one-crossing variant) on the
+    axial geometries; it must meet the same bar as the default cell-interval kernel."""
+    import os
+    import subprocess
+    import sys
+    code = r"""
+import numpy as np, torch, sys
+sys.path.insert(0, '.')
+from tests import geometries as G
+from oracle import oracle as O
+from tigre_b200 import _native as N, projectors as P
+for mk, ang in ((G.c1_geometry, G.angles(40)), (G.odd_geometry, G.angles(23, full=np.pi * 1.3))):
+    geo = mk()
+    img = G.phantom(tuple(int(v) for v in geo.nVoxel), seed=4)
+    plan = N.get_plan(N.checked_geometry(geo, ang), 0)
+    got = P.ax(torch.from_numpy(img).cuda(), plan, 'Siddon').cpu().numpy()
+    mx, l2 = G.rel_err(got, O.ax(img, geo, ang, 'Siddon'))
+    assert mx <= 1e-5 and l2 <= 1e-5, (mx, l2)
+    assert plan.status() == 0
+print('ok')
+"""
+    env = dict(os.environ, TIGRE_B200_NO_CELLS="1")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env,
+                       cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))), timeout=600)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr

@@ -58,6 +58,7 @@ _lock = threading.Lock()
 _SIGS = {
     "tigre_last_error": (C.c_char_p, []),
     "tigre_version": (C.c_int, []),
+    "tigre_launch_count": (C.c_ulonglong, []),
     "tigre_siddon_ray_projection": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                               C.c_int]),
     "tigre_interpolation_projection": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,

@@ -62,9 +62,12 @@ int tigre_ax(TigrePlan* plan, const void* d_vol, int vdt, void* d_proj, int pdt,
     const size_t es = dtype_size(vdt);
     int rc = TIGRE_SUCCESS;
     if (projector == TIGRE_PROJ_SIDDON && plan->columns) {
-        void* s = plan_scratch(plan, (size_t)d.nX * d.nY * (d.nZ + 2) * es, st, &rc);
+        // z-fast working copy; the cell-interval kernel needs deeper zero pads
+        const int zpad = plan->cells_zpad > 0 ? plan->cells_zpad : 1;
+        void* s = plan_scratch(plan, (size_t)d.nX * d.nY * (d.nZ + 2 * zpad) * es, st, &rc);
         if (rc) return rc;
-        if ((rc = launch_make_zfast(d_vol, vdt, s, d.nX, d.nY, d.nZ, st))) return rc;
+        if ((rc = launch_make_zfast(d_vol, vdt, s, d.nX, d.nY, d.nZ, zpad, st))) return rc;
+        if (plan->cells_zpad > 0) return launch_siddon_cells(plan, s, vdt, d_proj, pdt, a0, a1, st);
         return launch_siddon_columns(plan, s, vdt, d_proj, pdt, a0, a1, st);
     }
     if (projector == TIGRE_PROJ_SIDDON) {

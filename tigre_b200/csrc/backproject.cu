@@ -217,7 +217,7 @@ int launch_backproject(TigrePlan* P, const void* proj_pad, int pdt, void* vol, i
     else if (pdt == TIGRE_BF16 && vdt == TIGRE_F32) launch_typed<__nv_bfloat16, float>(a, matched, ax, st);
     else if (pdt == TIGRE_F16 && vdt == TIGRE_F32) launch_typed<__half, float>(a, matched, ax, st);
     else return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype pair for backprojection");
-    TIGRE_CUDA(cudaGetLastError());
+    TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
 

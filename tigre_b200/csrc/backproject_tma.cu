@@ -397,7 +397,7 @@ int launch_typed(const CUtensorMap& tm, const BPKArgs& a, bool matched, bool axi
     auto go = [&](auto kern) -> int {
         TIGRE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<grid, TXY * TXY, smem, st>>>(tm, a);
-        TIGRE_CUDA(cudaGetLastError());
+        TIGRE_LAUNCHED();
         return TIGRE_SUCCESS;
     };
     if (matched) return axial ? go(bp_tma_kernel<TP, TV, true, true>) : go(bp_tma_kernel<TP, TV, true, false>);

@@ -101,7 +101,7 @@ int tigre_sumsq(const void* d_x, int dtype, long n, double* d_out, void* stream)
     if (n == 0) return TIGRE_SUCCESS;
     cudaStream_t st = (cudaStream_t)stream;
     TIGRE_DISPATCH_DTYPE(dtype, T, { sumsq_kernel<T><<<grid_for(n), 256, 0, st>>>((const T*)d_x, n, d_out); });
-    TIGRE_CUDA(cudaGetLastError());
+    TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
 
@@ -109,7 +109,7 @@ int tigre_dot(const float* d_x, const float* d_y, long n, double* d_out, void* s
     if (n < 0 || !d_out) return fail(TIGRE_ERR_BAD_ASSERT, "bad dot arguments");
     if (n == 0) return TIGRE_SUCCESS;
     dot_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(d_x, d_y, n, d_out);
-    TIGRE_CUDA(cudaGetLastError());
+    TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
 
@@ -118,7 +118,7 @@ int tigre_cgls_step(float* d_x, const float* d_p, long nvol, float* d_r, const f
     if (nvol < 0 || nproj < 0 || !d_num || !d_den) return fail(TIGRE_ERR_BAD_ASSERT, "bad cgls_step arguments");
     cgls_step_kernel<<<grid_for(std::max(nvol, nproj)), 256, 0, (cudaStream_t)stream>>>(d_x, d_p, nvol, d_r, d_q,
                                                                                         nproj, d_num, d_den, d_rr);
-    TIGRE_CUDA(cudaGetLastError());
+    TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
 
@@ -126,7 +126,7 @@ int tigre_cgls_direction(float* d_p, const float* d_s, long n, const double* d_n
                          void* stream) {
     if (n < 0 || !d_num || !d_den) return fail(TIGRE_ERR_BAD_ASSERT, "bad cgls_direction arguments");
     cgls_dir_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(d_p, d_s, n, d_num, d_den);
-    TIGRE_CUDA(cudaGetLastError());
+    TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
 
@@ -139,7 +139,7 @@ int tigre_convert(const void* d_src, int sdt, void* d_dst, int ddt, long n, void
             convert_kernel<TS, TD><<<grid_for(n), 256, 0, st>>>((const TS*)d_src, (TD*)d_dst, n);
         });
     });
-    TIGRE_CUDA(cudaGetLastError());
+    TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
 

@@ -144,7 +144,7 @@ int launch_interp(TigrePlan* P, const void* vol_x, const void* vol_y, int vdt, v
         else if (vdt == TIGRE_BF16 && pdt == TIGRE_F32) launch_typed<__nv_bfloat16, float>(ac, nearest, grid, block, st);
         else if (vdt == TIGRE_F16 && pdt == TIGRE_F32) launch_typed<__half, float>(ac, nearest, grid, block, st);
         else return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype pair for interpolated projection");
-        TIGRE_CUDA(cudaGetLastError());
+        TIGRE_LAUNCHED();
     }
     return TIGRE_SUCCESS;
 }

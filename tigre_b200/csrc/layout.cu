@@ -52,15 +52,16 @@ __global__ void make_layout_kernel(const T* __restrict__ src, T* __restrict__ ds
     }
 }
 
-// z-fastest copy: dst (X, Y, Z+2), dst[(x*Y + y)*(Z+2) + zp] = src(z = zp-1, y, x), zeros at zp = 0, Z+1.
+// z-fastest copy with P zero slices before and after each z-run: dst (X, Y, Z+2P),
+// dst[(x*Y + y)*(Z+2P) + zp] = src(z = zp-P, y, x), zero where zp-P is outside [0, Z).
 // One y per block row of the grid; a 32x32 (zp, x) tile goes through shared memory.
 template <typename T>
-__global__ void make_zfast_kernel(const T* __restrict__ src, T* __restrict__ dst, int nX, int nY, int nZ) {
+__global__ void make_zfast_kernel(const T* __restrict__ src, T* __restrict__ dst, int nX, int nY, int nZ, int P) {
     __shared__ T tile[TILE][TILE + 1];
-    const int ZP = nZ + 2;
+    const int ZP = nZ + 2 * P;
     const int zp0 = blockIdx.x * TILE, x0 = blockIdx.y * TILE, y = blockIdx.z;
     for (int j = threadIdx.y; j < TILE; j += blockDim.y) {
-        const int zp = zp0 + j, x = x0 + threadIdx.x, z = zp - 1;
+        const int zp = zp0 + j, x = x0 + threadIdx.x, z = zp - P;
         T v = from_f32<T>(0.f);
         if (z >= 0 && z < nZ && x < nX) v = src[((size_t)z * nY + y) * nX + x];
         tile[j][threadIdx.x] = v;
@@ -104,7 +105,7 @@ int launch_repitch_projections(const void* src, int dtype, void* dst, int nA, in
     const long want = (rows * pitch + 255) / 256;
     const int grid = (int)std::min<long>(want, 148L * 32);
     TIGRE_DISPATCH_DTYPE(dtype, T, { repitch_kernel<T><<<grid, 256, 0, st>>>((const T*)src, (T*)dst, nU, pitch, rows); });
-    TIGRE_CUDA(cudaGetLastError());
+    TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
 
@@ -119,15 +120,17 @@ int launch_make_layout(const void* src, int dtype, void* dst, int nX, int nY, in
         else
             make_layout_kernel<T, 1><<<grid, block, 0, st>>>((const T*)src, (T*)dst, nX, nY, nZ, pad_lo, pad_hi);
     });
-    TIGRE_CUDA(cudaGetLastError());
+    TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
 
-int launch_make_zfast(const void* src, int dtype, void* dst, int nX, int nY, int nZ, cudaStream_t st) {
+int launch_make_zfast(const void* src, int dtype, void* dst, int nX, int nY, int nZ, int zpad, cudaStream_t st) {
     dim3 block(TILE, 8);
-    dim3 grid((nZ + 2 + TILE - 1) / TILE, (nX + TILE - 1) / TILE, nY);
-    TIGRE_DISPATCH_DTYPE(dtype, T, { make_zfast_kernel<T><<<grid, block, 0, st>>>((const T*)src, (T*)dst, nX, nY, nZ); });
-    TIGRE_CUDA(cudaGetLastError());
+    dim3 grid((nZ + 2 * zpad + TILE - 1) / TILE, (nX + TILE - 1) / TILE, nY);
+    TIGRE_DISPATCH_DTYPE(dtype, T, {
+        make_zfast_kernel<T><<<grid, block, 0, st>>>((const T*)src, (T*)dst, nX, nY, nZ, zpad);
+    });
+    TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
 
@@ -139,7 +142,7 @@ int launch_pad_projections(const void* src, int dtype, void* dst, int nA, int nV
     TIGRE_DISPATCH_DTYPE(dtype, T, {
         pad_projections_kernel<T><<<grid, block, 0, st>>>((const T*)src, (T*)dst, nV, nU, total);
     });
-    TIGRE_CUDA(cudaGetLastError());
+    TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
 

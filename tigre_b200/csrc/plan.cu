@@ -11,6 +11,7 @@
 //                     Common/CUDA/voxel_backprojection.cu:762-898
 // The reference evaluates most of them in float; here everything is double.
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -25,6 +26,12 @@ namespace tigre {
 static thread_local std::string g_last_error;
 
 void set_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}
+
+void note_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int fail(int code, const std::string& msg) {
     set_error(msg);
@@ -91,6 +98,48 @@ Rot3 euler_zyz_T(double a, double t, double p) {
 inline double at(const float* a, int i) { return a ? (double)a[i] : 0.0; }
 
 }  // namespace
+
+// Exact bounds for the cell-interval Siddon kernel, evaluated with the kernel's own FP64 ray
+// setup for every view and detector column: within one column the z component of the ray
+// is linear in the row, so its extremes are the first and the last row.
+void cells_bounds(TigrePlan* plan) {
+    const Dims& d = plan->d;
+    double slope = 0.0, span = 0.0;
+    for (const FrameSiddon& f : plan->h_siddon) {
+        for (int u = 0; u < d.nU; ++u) {
+            double rx = std::fma((double)u, f.du[0], f.o[0]) - f.s[0];
+            double ry = std::fma((double)u, f.du[1], f.o[1]) - f.s[1];
+            if (std::fabs(rx) < 0.001) rx = 0.0;
+            if (std::fabs(ry) < 0.001) ry = 0.0;
+            double am = -1e300, aM = 1e300;
+            bool miss = false;
+            if (rx != 0.0) {
+                const double i = 1.0 / rx, a0 = -f.s[0] * i, a1 = ((double)d.nX - f.s[0]) * i;
+                am = std::fmax(am, std::fmin(a0, a1)); aM = std::fmin(aM, std::fmax(a0, a1));
+            } else if (f.s[0] < 0.0 || f.s[0] > (double)d.nX) miss = true;
+            if (ry != 0.0) {
+                const double i = 1.0 / ry, a0 = -f.s[1] * i, a1 = ((double)d.nY - f.s[1]) * i;
+                am = std::fmax(am, std::fmin(a0, a1)); aM = std::fmin(aM, std::fmax(a0, a1));
+            } else if (f.s[1] < 0.0 || f.s[1] > (double)d.nY) miss = true;
+            if (miss || !(am < aM)) continue;
+            const double dom = std::max(std::fabs(rx), std::fabs(ry));
+            for (int e = 0; e < 2; ++e) {
+                const double pv = e ? 0.0 : (double)(d.nV - 1);
+                double rz = std::fma(pv, f.dv[2], std::fma((double)u, f.du[2], f.o[2])) - f.s[2];
+                if (std::fabs(rz) < 0.001) rz = 0.0;
+                slope = std::max(slope, dom > 0.0 ? std::fabs(rz) / dom : 1e30);
+                span = std::max(span, (aM - am) * std::fabs(rz));
+            }
+        }
+    }
+    plan->cells_slope_max = slope;
+    plan->cells_zspan_max = span;
+    // one z crossing per xy cell at most (z change per cell < 1, with margin), and pads that
+    // stay a modest multiple of the volume
+    const double pad = std::ceil(span) + 3.0;
+    const bool ok = slope < 0.9 && pad <= 2.0 * d.nZ + 256.0 && std::getenv("TIGRE_B200_NO_CELLS") == nullptr;
+    plan->cells_zpad = ok ? (int)pad : 0;
+}
 
 int compute_frames(const TigreGeometry* g, const float* angles, int nangles, TigrePlan* plan) {
     TIGRE_CHECK(g != nullptr && angles != nullptr, "null geometry or angles");
@@ -225,6 +274,7 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
     }
     plan->axial = axial;
     plan->columns = columns && std::getenv("TIGRE_B200_GENERIC_SIDDON") == nullptr;
+    if (plan->columns) cells_bounds(plan);
 
     // ---- staged backprojector constants and patch box ----
     plan->h_bpk.resize(nangles);
@@ -329,6 +379,7 @@ extern "C" {
 const char* tigre_last_error(void) { return g_last_error.c_str(); }
 
 int tigre_version(void) { return 100; }
+unsigned long long tigre_launch_count(void) { return tigre::g_launches.load(std::memory_order_relaxed); }
 
 int tigre_plan_create(const TigreGeometry* geo, const float* angles, int nangles, int device, TigrePlan** out) {
     if (!out) return fail(TIGRE_ERR_BAD_ASSERT, "null output plan pointer");

@@ -37,6 +37,8 @@ struct SiddonArgs {
     int nX, nY, nZ, nU, nV;
     double dVX, dVY, dVZ;
     unsigned long long* count;   // segment-count mode
+    int zpad;                    // zero slices before and after each z-run of the z-fast copy
+    int* status;                 // plan status word (bit 1: a ray outside the host's z bound)
 };
 
 constexpr float kInf = __builtin_huge_valf();
@@ -277,7 +279,7 @@ __global__ void __launch_bounds__(128, 6) siddon_columns_kernel(SiddonArgs p) {
         tz[r] = tz0[r];
     }
     const TV* __restrict__ vol = (const TV*)p.vol_x;
-    const int ZP = p.nZ + 2;
+    const int ZP = p.nZ + 2 * p.zpad;
     int cidx = ax.i * p.nY + ay.i;
     const int dcx = ax.step * p.nY, dcy = ay.step;
     int remx = ax.rem, remy = ay.rem;
@@ -353,12 +355,169 @@ __global__ void __launch_bounds__(128, 6) siddon_columns_kernel(SiddonArgs p) {
     }
 }
 
+// Cell-interval Siddon, for plans whose rays change z by less than one slice per xy
+// cell (the host checks this exactly for every ray).  Same warp organisation as
+// siddon_columns_kernel, but the z state is not stepped: with z(alpha) = zA + alpha*rz
+// the slice at the end b of each xy cell is floor(z(b)), and since at most one z plane
+// lies inside the cell, its contribution is
+//     seg * v(z_start) + (b - alpha_k) * (v(z_end) - v(z_start)),
+// where alpha_k is the crossing, taken in alpha space from the crossing count
+// (alpha_k = tz0 + (z_end - q) / rz, exact small integers in the difference).  Without a
+// crossing v(z_end) = v(z_start) and the second term is zero, so every cell of every row
+// runs the same branch-free code on the FMA pipe, two rows at a time in packed FP32x2.
+// The floor is a round-toward-zero add of 1.5*2^23 (z is kept positive by the pads), and
+// its float bits index the column directly.  The pads (at least the largest z extent of
+// any ray inside the xy box, from the host) make every index valid without clamping:
+// a ray whose z range misses the volume reads one zero slice.
+constexpr float kMagic = 12582912.0f;          // 1.5 * 2^23
+constexpr unsigned kMagicBits = 0x4B400000u;   // its bit pattern
+
+__device__ __forceinline__ float2 pk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 pk(float a) { return make_float2(a, a); }
+
+template <typename TV>
+__device__ __forceinline__ float ldz(uintptr_t cb, float t) {
+    return ldg_f<TV>(reinterpret_cast<const TV*>(cb + (uintptr_t)__float_as_uint(t) * sizeof(TV)));
+}
+
+template <typename TV, typename TP, int R>
+__global__ void __launch_bounds__(128, 6) siddon_cells_kernel(SiddonArgs p) {
+    static_assert(R % 2 == 0, "rows are processed in pairs");
+    constexpr int H = R / 2;
+    const int lane = threadIdx.x & 31;
+    const int u = blockIdx.x * 4 + (threadIdx.x >> 5);
+    const int la = blockIdx.y;
+    if (u >= p.nU) return;
+    const FrameSiddon& F = p.frames[p.a0 + la];
+    const int vbase = blockIdx.z * (32 * R) + lane;
+    TP* out = (TP*)p.proj + (size_t)la * p.nV * p.nU + u;
+    // ---- shared xy ray ----
+    double rx = fma((double)u, F.du[0], F.o[0]) - F.s[0];
+    double ry = fma((double)u, F.du[1], F.o[1]) - F.s[1];
+    if (fabs(rx) < 0.001) rx = 0.0;   // Siddon_projection.cu:156-159
+    if (fabs(ry) < 0.001) ry = 0.0;
+    double am = -1e300, aM = 1e300;
+    bool miss = false;
+    if (rx != 0.0) {
+        const double i = 1.0 / rx, a0 = -F.s[0] * i, a1 = ((double)p.nX - F.s[0]) * i;
+        am = fmax(am, fmin(a0, a1)); aM = fmin(aM, fmax(a0, a1));
+    } else if (F.s[0] < 0.0 || F.s[0] > (double)p.nX) miss = true;
+    if (ry != 0.0) {
+        const double i = 1.0 / ry, a0 = -F.s[1] * i, a1 = ((double)p.nY - F.s[1]) * i;
+        am = fmax(am, fmin(a0, a1)); aM = fmin(aM, fmax(a0, a1));
+    } else if (F.s[1] < 0.0 || F.s[1] > (double)p.nY) miss = true;
+    if (miss || !(am < aM)) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int v = vbase + 32 * r;
+            if (v < p.nV) out[(size_t)v * p.nU] = from_f32<TP>(0.f);
+        }
+        return;
+    }
+    const AxisSetup ax = axis_setup(F.s[0], rx, am, aM, p.nX);
+    const AxisSetup ay = axis_setup(F.s[1], ry, am, aM, p.nY);
+    const int ncells = 1 + (int)ax.ncross + (int)ay.ncross;
+    const double Td = aM - am;
+    const float T = (float)Td;
+    const double P = (double)p.zpad;
+    // ---- per-row z state, rows (2h, 2h+1) packed in .x/.y ----
+    float2 zA[H], rz[H], nm[H], nQ[H], ntz0[H], sum[H], t0[H];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int v = min(vbase + 32 * r, p.nV - 1);
+        const double pv = (double)(p.nV - 1 - v);
+        double rzd = fma(pv, F.dv[2], fma((double)u, F.du[2], F.o[2])) - F.s[2];
+        if (fabs(rzd) < 0.001) rzd = 0.0;
+        const double za = fma(am, rzd, F.s[2]) + P;   // z + pad at the xy entry
+        const double zb = fma(Td, rzd, za);           // ... and at the xy exit
+        const double lo = fmin(za, zb), hi = fmax(za, zb);
+        bool live = hi > P && lo < P + (double)p.nZ;
+        if (live && hi - lo > P - 1.5) {              // beyond the host's bound: not expected
+            live = false;
+            if (p.status) atomicOr(p.status, 2);
+        }
+        float zaf = (float)(P - 0.5), rzf = 0.f, m = 0.f, q = 0.f, tz = 0.f;
+        if (live) {
+            zaf = (float)za;
+            rzf = (float)rzd;
+            const float zs = __fadd_rz(zaf, kMagic) - kMagic;   // floor(zA) as the loop computes it
+            if (rzd > 0.0) {
+                q = zs + 1.f;
+                tz = (float)(((double)zs + 1.0 - za) / rzd);
+                m = (float)(1.0 / rzd);
+            } else if (rzd < 0.0) {
+                q = zs - 1.f;
+                tz = (float)(((double)zs - za) / rzd);
+                m = (float)(1.0 / rzd);
+            }
+        }
+        const float t = __fadd_rz(zaf, kMagic);
+        if (r & 1) {
+            zA[r >> 1].y = zaf; rz[r >> 1].y = rzf; nm[r >> 1].y = -m; nQ[r >> 1].y = -(kMagic + q);
+            ntz0[r >> 1].y = -tz; sum[r >> 1].y = 0.f; t0[r >> 1].y = t;
+        } else {
+            zA[r >> 1].x = zaf; rz[r >> 1].x = rzf; nm[r >> 1].x = -m; nQ[r >> 1].x = -(kMagic + q);
+            ntz0[r >> 1].x = -tz; sum[r >> 1].x = 0.f; t0[r >> 1].x = t;
+        }
+    }
+    const uintptr_t vb = (uintptr_t)p.vol_x - (uintptr_t)kMagicBits * sizeof(TV);
+    const uintptr_t colb = (uintptr_t)(p.nZ + 2 * p.zpad) * sizeof(TV);
+    int cidx = ax.i * p.nY + ay.i;
+    const int dcx = ax.step * p.nY, dcy = ay.step;
+    int remx = ax.rem, remy = ay.rem;
+    float tx = ax.t0, ty = ay.t0, kx = 0.f, ky = 0.f;
+    float a = 0.f;
+#pragma unroll 1
+    for (int c = 0; c < ncells; ++c) {
+        const float b = fminf(fminf(tx, ty), T);
+        const float2 b2 = pk(b), seg2 = pk(b - a);
+        const uintptr_t cb = vb + (uintptr_t)cidx * colb;
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            const float2 zf = __ffma2_rn(b2, rz[h], zA[h]);
+            const float2 t1 = __fadd2_rz(zf, pk(kMagic));             // kMagic + floor(z(b))
+            const float2 kq = __fadd2_rn(t1, nQ[h]);                  // z_end - q, exact
+            const float2 d = __fadd2_rn(b2, __ffma2_rn(kq, nm[h], ntz0[h]));   // b - alpha_k
+            const float2 v0 = pk(ldz<TV>(cb, t0[h].x), ldz<TV>(cb, t0[h].y));
+            const float2 v1 = pk(ldz<TV>(cb, t1.x), ldz<TV>(cb, t1.y));
+            sum[h] = __ffma2_rn(seg2, v0, sum[h]);
+            sum[h] = __ffma2_rn(d, __ffma2_rn(v0, pk(-1.f), v1), sum[h]);
+            t0[h] = t1;
+        }
+        a = b;
+        const bool stepx = tx <= ty;
+        cidx += stepx ? dcx : dcy;
+        if (stepx) {
+            kx += 1.f;
+            tx = (--remx > 0) ? fmaf(kx, ax.dt, ax.t0) : kInf;
+        } else {
+            ky += 1.f;
+            ty = (--remy > 0) ? fmaf(ky, ay.dt, ay.t0) : kInf;
+        }
+    }
+    const double lxy = rx * rx * p.dVX * p.dVX + ry * ry * p.dVY * p.dVY;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int v = vbase + 32 * r;
+        if (v < p.nV) {
+            const double pv = (double)(p.nV - 1 - v);
+            double rzd = fma(pv, F.dv[2], fma((double)u, F.du[2], F.o[2])) - F.s[2];
+            if (fabs(rzd) < 0.001) rzd = 0.0;
+            const float len = (float)sqrt(lxy + rzd * rzd * p.dVZ * p.dVZ);
+            const float sr = (r & 1) ? sum[r >> 1].y : sum[r >> 1].x;
+            out[(size_t)v * p.nU] = from_f32<TP>(sr * len);
+        }
+    }
+}
+
 SiddonArgs make_args(TigrePlan* P, int a0) {
     SiddonArgs a{};
     a.frames = P->d_siddon;
     a.a0 = a0;
     a.nX = P->d.nX; a.nY = P->d.nY; a.nZ = P->d.nZ; a.nU = P->d.nU; a.nV = P->d.nV;
     a.dVX = P->d.dVX; a.dVY = P->d.dVY; a.dVZ = P->d.dVZ;
+    a.zpad = 1;
+    a.status = P->d_status;
     return a;
 }
 
@@ -391,7 +550,7 @@ int launch_siddon(TigrePlan* P, const void* vol_x, const void* vol_y, int vdt, v
             siddon_kernel<float, __nv_bfloat16><<<grid, block, 0, st>>>(ac);
         else if (vdt == TIGRE_F32 && pdt == TIGRE_F16) siddon_kernel<float, __half><<<grid, block, 0, st>>>(ac);
         else return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype pair for Siddon");
-        TIGRE_CUDA(cudaGetLastError());
+        TIGRE_LAUNCHED();
     }
     return TIGRE_SUCCESS;
 }
@@ -432,7 +591,40 @@ int launch_siddon_columns(TigrePlan* P, const void* vol_z, int vdt, void* proj, 
         else if (vdt == TIGRE_F32 && pdt == TIGRE_BF16) launch_columns_typed<float, __nv_bfloat16>(ac, R, single, grid, st);
         else if (vdt == TIGRE_F32 && pdt == TIGRE_F16) launch_columns_typed<float, __half>(ac, R, single, grid, st);
         else return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype pair for Siddon");
-        TIGRE_CUDA(cudaGetLastError());
+        TIGRE_LAUNCHED();
+    }
+    return TIGRE_SUCCESS;
+}
+
+template <typename TV, typename TP>
+static void launch_cells_typed(const SiddonArgs& a, int rows_per_thread, dim3 grid, cudaStream_t st) {
+    if (rows_per_thread == 4) siddon_cells_kernel<TV, TP, 4><<<grid, 128, 0, st>>>(a);
+    else siddon_cells_kernel<TV, TP, 2><<<grid, 128, 0, st>>>(a);
+}
+
+int launch_siddon_cells(TigrePlan* P, const void* vol_z, int vdt, void* proj, int pdt, int a0, int a1,
+                        cudaStream_t st) {
+    SiddonArgs a = make_args(P, a0);
+    a.vol_x = vol_z;
+    a.proj = proj;
+    a.zpad = P->cells_zpad;
+    const int nv = P->d.nV;
+    const int R = nv >= 256 ? 4 : 2;
+    const int na = a1 - a0;
+    for (int c = 0; c < na; c += 65535) {
+        SiddonArgs ac = a;
+        ac.a0 = a0 + c;
+        ac.proj = (char*)proj + (size_t)c * P->d.nU * P->d.nV * dtype_size(pdt);
+        dim3 grid((P->d.nU + 3) / 4, std::min(65535, na - c), (nv + 32 * R - 1) / (32 * R));
+        if (vdt == TIGRE_F32 && pdt == TIGRE_F32) launch_cells_typed<float, float>(ac, R, grid, st);
+        else if (vdt == TIGRE_BF16 && pdt == TIGRE_BF16) launch_cells_typed<__nv_bfloat16, __nv_bfloat16>(ac, R, grid, st);
+        else if (vdt == TIGRE_F16 && pdt == TIGRE_F16) launch_cells_typed<__half, __half>(ac, R, grid, st);
+        else if (vdt == TIGRE_BF16 && pdt == TIGRE_F32) launch_cells_typed<__nv_bfloat16, float>(ac, R, grid, st);
+        else if (vdt == TIGRE_F16 && pdt == TIGRE_F32) launch_cells_typed<__half, float>(ac, R, grid, st);
+        else if (vdt == TIGRE_F32 && pdt == TIGRE_BF16) launch_cells_typed<float, __nv_bfloat16>(ac, R, grid, st);
+        else if (vdt == TIGRE_F32 && pdt == TIGRE_F16) launch_cells_typed<float, __half>(ac, R, grid, st);
+        else return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype pair for Siddon");
+        TIGRE_LAUNCHED();
     }
     return TIGRE_SUCCESS;
 }
@@ -448,7 +640,7 @@ int launch_siddon_count(TigrePlan* P, int a0, int a1, unsigned long long* d_tota
         ac.a0 = a0 + c;
         grid.z = std::min(65535, na - c);
         siddon_count_kernel<<<grid, block, 0, st>>>(ac);
-        TIGRE_CUDA(cudaGetLastError());
+        TIGRE_LAUNCHED();
     }
     return TIGRE_SUCCESS;
 }

@@ -17,6 +17,15 @@ namespace tigre {
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
+// process-wide count of kernels launched by this library (tigre_launch_count)
+void note_launches(unsigned long long n);
+
+// after a kernel launch: check the launch and count it
+#define TIGRE_LAUNCHED()                   \
+    do {                                   \
+        TIGRE_CUDA(cudaGetLastError());    \
+        ::tigre::note_launches(1);         \
+    } while (0)
 
 #define TIGRE_CUDA(call)                                     \
     do {                                                     \
@@ -107,6 +116,11 @@ struct TigrePlan {
     bool axial = false;          // every BP frame has dz.x == dz.y == 0 (u constant along z)
     bool columns = false;        // every Siddon frame has dv.x == dv.y == 0 (detector v parallel to z)
     double column_slope_max = 0; // max over rays of |rz| / max(|rx|, |ry|): z change per xy cell
+    // cell-interval Siddon: exact maxima over all rays (FP64, the kernel's own ray setup) of the
+    // z change per xy cell and of the z extent of the ray inside the xy box; cells_zpad zero
+    // slices before and after each z-run of the working copy cover that extent
+    double cells_slope_max = 0, cells_zspan_max = 0;
+    int cells_zpad = 0;          // 0: the cell-interval kernel is not usable for this plan
     std::vector<tigre::FrameBPK> h_bpk;
     tigre::FrameBPK* d_bpk = nullptr;
     int bp_box_u = 0, bp_box_v = 0;   // TMA patch box of the staged backprojector (0: not usable)
@@ -125,11 +139,13 @@ void* plan_scratch(TigrePlan* plan, size_t bytes, cudaStream_t st, int* rc);
 int launch_make_layout(const void* src, int dtype, void* dst, int nX, int nY, int nZ, int layout, int pad_lo,
                        int pad_hi, cudaStream_t st);
 int launch_pad_projections(const void* src, int dtype, void* dst, int nA, int nV, int nU, cudaStream_t st);
-int launch_make_zfast(const void* src, int dtype, void* dst, int nX, int nY, int nZ, cudaStream_t st);
+int launch_make_zfast(const void* src, int dtype, void* dst, int nX, int nY, int nZ, int zpad, cudaStream_t st);
 
 int launch_siddon(TigrePlan* p, const void* vol_x, const void* vol_y, int vdt, void* proj, int pdt, int a0, int a1,
                   cudaStream_t st);
 int launch_siddon_count(TigrePlan* p, int a0, int a1, unsigned long long* d_total, cudaStream_t st);
+int launch_siddon_cells(TigrePlan* p, const void* vol_z, int vdt, void* proj, int pdt, int a0, int a1,
+                        cudaStream_t st);
 int launch_siddon_columns(TigrePlan* p, const void* vol_z, int vdt, void* proj, int pdt, int a0, int a1,
                           cudaStream_t st);
 int launch_interp(TigrePlan* p, const void* vol_x, const void* vol_y, int vdt, void* proj, int pdt, int a0, int a1,

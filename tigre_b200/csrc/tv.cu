@@ -167,7 +167,7 @@ int tigre_tv_gradient(const void* d_img, int dtype, float* d_grad, long nx, long
     TVDims d{(int)nx, (int)ny, (int)nz};
     const size_t n = (size_t)nx * ny * nz;
     tv_grad_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const float*)d_img, d_grad, d);
-    TIGRE_CUDA(cudaGetLastError());
+    TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
 
@@ -177,7 +177,7 @@ int tigre_tv_value(const void* d_img, int dtype, long nx, long ny, long nz, doub
     TVDims d{(int)nx, (int)ny, (int)nz};
     const size_t n = (size_t)nx * ny * (nz + 1);
     tv_value_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const float*)d_img, d, d_out);
-    TIGRE_CUDA(cudaGetLastError());
+    TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
 
@@ -205,6 +205,7 @@ int tigre_tv_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha
     if (cur != (float*)d_img) TIGRE_CUDA(cudaMemcpyAsync(d_img, cur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
     TIGRE_CUDA(cudaFreeAsync(sums, st));
     TIGRE_CUDA(cudaGetLastError());
+    note_launches(2ull * (unsigned long long)max_iter);
     return TIGRE_SUCCESS;
 }
 
@@ -276,5 +277,6 @@ extern "C" int tigre_tv_pocs_noalloc(void* d_img, int dtype, long nx, long ny, l
     }
     if (cur != (float*)d_img) TIGRE_CUDA(cudaMemcpyAsync(d_img, cur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
     TIGRE_CUDA(cudaGetLastError());
+    note_launches(2ull * (unsigned long long)max_iter);
     return TIGRE_SUCCESS;
 }
