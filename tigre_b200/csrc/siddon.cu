@@ -381,7 +381,7 @@ __device__ __forceinline__ float ldz(uintptr_t cb, float t) {
 }
 
 template <typename TV, typename TP, int R>
-__global__ void __launch_bounds__(128, 6) siddon_cells_kernel(SiddonArgs p) {
+__global__ void __launch_bounds__(128, 5) siddon_cells_kernel(SiddonArgs p) {
     static_assert(R % 2 == 0, "rows are processed in pairs");
     constexpr int H = R / 2;
     const int lane = threadIdx.x & 31;
@@ -467,21 +467,26 @@ __global__ void __launch_bounds__(128, 6) siddon_cells_kernel(SiddonArgs p) {
     int remx = ax.rem, remy = ay.rem;
     float tx = ax.t0, ty = ay.t0, kx = 0.f, ky = 0.f;
     float a = 0.f;
-#pragma unroll 1
-    for (int c = 0; c < ncells; ++c) {
+    // Software pipeline over cells: front() of cell k+1 (its bounds, floors and the four loads
+    // per row pair) is issued before back() of cell k (the accumulation), so the loads of one
+    // cell are in flight while the previous one is summed.  Two state sets, A and B, alternate.
+    struct Cell {
+        float seg;
+        float2 d[H], v0[H], v1[H];
+    };
+    auto front = [&](Cell& C) {
         const float b = fminf(fminf(tx, ty), T);
-        const float2 b2 = pk(b), seg2 = pk(b - a);
+        const float2 b2 = pk(b);
+        C.seg = b - a;
         const uintptr_t cb = vb + (uintptr_t)cidx * colb;
 #pragma unroll
         for (int h = 0; h < H; ++h) {
             const float2 zf = __ffma2_rn(b2, rz[h], zA[h]);
-            const float2 t1 = __fadd2_rz(zf, pk(kMagic));             // kMagic + floor(z(b))
-            const float2 kq = __fadd2_rn(t1, nQ[h]);                  // z_end - q, exact
-            const float2 d = __fadd2_rn(b2, __ffma2_rn(kq, nm[h], ntz0[h]));   // b - alpha_k
-            const float2 v0 = pk(ldz<TV>(cb, t0[h].x), ldz<TV>(cb, t0[h].y));
-            const float2 v1 = pk(ldz<TV>(cb, t1.x), ldz<TV>(cb, t1.y));
-            sum[h] = __ffma2_rn(seg2, v0, sum[h]);
-            sum[h] = __ffma2_rn(d, __ffma2_rn(v0, pk(-1.f), v1), sum[h]);
+            const float2 t1 = __fadd2_rz(zf, pk(kMagic));                       // kMagic + floor(z(b))
+            const float2 kq = __fadd2_rn(t1, nQ[h]);                            // z_end - q, exact
+            C.d[h] = __fadd2_rn(b2, __ffma2_rn(kq, nm[h], ntz0[h]));            // b - alpha_k
+            C.v0[h] = pk(ldz<TV>(cb, t0[h].x), ldz<TV>(cb, t0[h].y));
+            C.v1[h] = pk(ldz<TV>(cb, t1.x), ldz<TV>(cb, t1.y));
             t0[h] = t1;
         }
         a = b;
@@ -494,6 +499,27 @@ __global__ void __launch_bounds__(128, 6) siddon_cells_kernel(SiddonArgs p) {
             ky += 1.f;
             ty = (--remy > 0) ? fmaf(ky, ay.dt, ay.t0) : kInf;
         }
+    };
+    auto back = [&](const Cell& C) {
+        const float2 seg2 = pk(C.seg);
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            sum[h] = __ffma2_rn(seg2, C.v0[h], sum[h]);
+            sum[h] = __ffma2_rn(C.d[h], __ffma2_rn(C.v0[h], pk(-1.f), C.v1[h]), sum[h]);
+        }
+    };
+    Cell A, B;
+    front(A);
+    int c = 1;
+#pragma unroll 1
+    while (true) {
+        if (c >= ncells) { back(A); break; }
+        front(B);
+        back(A);
+        if (++c >= ncells) { back(B); break; }
+        front(A);
+        back(B);
+        ++c;
     }
     const double lxy = rx * rx * p.dVX * p.dVX + ry * ry * p.dVY * p.dVY;
 #pragma unroll
