@@ -20,6 +20,7 @@
 // A (block, view) whose footprint does not fit the box (possible for strongly
 // magnified geometries) falls back to bounds-checked global loads.
 
+#include <type_traits>
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -31,8 +32,8 @@
 namespace tigre {
 namespace {
 
-constexpr int TXY = 16;   // columns per block edge
-constexpr int VZ = 16;    // slices per thread
+constexpr int TXY = kBpTile;   // columns per block edge
+constexpr int VZ = kBpSlices;  // slices per thread
 constexpr unsigned kWaitLimit = 1u << 16;   // ~ a few ms with the back-off below
 
 struct BPKArgs {
@@ -86,7 +87,7 @@ __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
 // a + t (b - a), two lanes at once
 __device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 t) {
-    return __ffma2_rn(t, __fadd2_rn(b, neg2(a)), a);
+    return __ffma2_rn(t, __ffma2_rn(a, f2(-1.f), b), a);
 }
 
 // texel-space (u - 0.5, v - 0.5) projection of voxel (x, y, z) for view frame F
@@ -177,7 +178,7 @@ __device__ __forceinline__ float global_sample(const BPKArgs& p, const TP* P, fl
 }
 
 template <typename TP, typename TV, bool MATCHED, bool AXIAL>
-__global__ void __launch_bounds__(TXY* TXY) bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, BPKArgs p) {
+__global__ void __launch_bounds__(TXY* TXY, 3) bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, BPKArgs p) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) unsigned long long bars[2];
     __shared__ int info[2][4];
@@ -189,7 +190,10 @@ __global__ void __launch_bounds__(TXY* TXY) bp_tma_kernel(const __grid_constant_
     const uint32_t buf0_u32 = smem_u32(buf0), buf1_u32 = smem_u32(buf1);
     const uint32_t rowb = (uint32_t)(p.BU * sizeof(TP));
     const int tid = threadIdx.x;
-    const int tx = tid & (TXY - 1), ty = tid / TXY;
+    // each warp covers an 8 x 4 patch of columns: at every view angle its 32 samples of one
+    // slice fall on a compact set of detector texels (few shared-memory wavefronts)
+    const int wid = tid >> 5, ln = tid & 31;
+    const int tx = (wid & 1) * 8 + (ln & 7), ty = (wid >> 1) * 4 + (ln >> 3);
     const int x0 = blockIdx.x * TXY, y0 = blockIdx.y * TXY, z0 = blockIdx.z * VZ;
     const int x = x0 + tx, y = y0 + ty;
     const bool active = x < p.nX && y < p.nY;
@@ -270,44 +274,53 @@ __global__ void __launch_bounds__(TXY* TXY) bp_tma_kernel(const __grid_constant_
                         ys = f2(rsqrtf(L2));
                         rs = f2(__fdividef(1.f, F.dsd * lsq));
                     }
+                    // the float bits of the floor below index the patch directly:
+                    // row address = bits * rowb + colb - 0x4B400000 * rowb (32-bit wrap)
+                    const uint32_t colb_m = colb - 0x4B400000u * rowb;
+                    const float2 ndsd2 = f2(-F.dsd);
+                    auto pairs = [&](auto clamp_tag) {
+                        constexpr bool CLAMP = decltype(clamp_tag)::value;
 #pragma unroll
-                    for (int k = 0; k < VZ; k += 2) {
-                        const float2 kk = f2((float)k, (float)(k + 1));
-                        float2 pv = __ffma2_rn(kk, vstep2, pv02);
-                        if (!inside) {
-                            pv.x = fminf(fmaxf(pv.x, 0.f), pvmax);
-                            pv.y = fminf(fmaxf(pv.y, 0.f), pvmax);
+                        for (int k = 0; k < VZ; k += 2) {
+                            const float2 kk = f2((float)k, (float)(k + 1));
+                            float2 pv = __ffma2_rn(kk, vstep2, pv02);
+                            if (CLAMP) {
+                                pv.x = fminf(fmaxf(pv.x, 0.f), pvmax);
+                                pv.y = fminf(fmaxf(pv.y, 0.f), pvmax);
+                            }
+                            // floor / fraction with packed arithmetic: pv >= 0 here, and at 1.5*2^23
+                            // the float spacing is 1, so a round-toward-zero add of 1.5*2^23 leaves
+                            // floor(pv) in the low mantissa bits; subtracting it back is exact
+                            const float2 t = __fadd2_rz(pv, f2(12582912.0f));
+                            const float2 fv = __ffma2_rn(__fadd2_rn(t, f2(-12582912.0f)), f2(-1.f), pv);
+                            const uint32_t aa = (uint32_t)__float_as_int(t.x) * rowb + colb_m;
+                            const uint32_t ab = (uint32_t)__float_as_int(t.y) * rowb + colb_m;
+                            const float2 r0 = f2(lds<TP>(aa), lds<TP>(ab)), r0r = f2(lds<TP>(aa + ES), lds<TP>(ab + ES));
+                            const float2 r1 = f2(lds<TP>(aa + rowb), lds<TP>(ab + rowb));
+                            const float2 r1r = f2(lds<TP>(aa + rowb + ES), lds<TP>(ab + rowb + ES));
+                            const float2 smp = lerp2(lerp2(r0, r0r, fu2), lerp2(r1, r1r, fu2), fv);
+                            float2 w = w2;
+                            if (MATCHED) {
+                                // w = L^3 / (DSD lsq); 1/sqrt(L^2) and 1/(DSD lsq) change by ~1e-4 relative per
+                                // slice, so one Newton-Raphson step from the previous pair's values
+                                // (y <- y (3 - x y^2)/2 ;  r <- r (2 - d r)) is accurate to ~1e-8
+                                const float2 vtex = __ffma2_rn(kk, vstep2, vt02);
+                                const float2 dz = __ffma2_rn(vtex, ddv2, dzc2);
+                                const float2 L2 = __ffma2_rn(dz, dz, cu22);
+                                const float2 rvz = __ffma2_rn(kk, dvz2, rz2);
+                                const float2 nden = __fmul2_rn(__ffma2_rn(rvz, rvz, cxy2), ndsd2);
+                                const float2 hl = __fmul2_rn(L2, f2(-0.5f));
+                                ys = __fmul2_rn(ys, __ffma2_rn(hl, __fmul2_rn(ys, ys), f2(1.5f)));
+                                rs = __fmul2_rn(rs, __ffma2_rn(nden, rs, f2(2.0f)));
+                                w = __fmul2_rn(__fmul2_rn(L2, L2), __fmul2_rn(ys, rs));
+                            }
+                            const float2 acc2 = __ffma2_rn(smp, w, f2(acc[k], acc[k + 1]));
+                            acc[k] = acc2.x;
+                            acc[k + 1] = acc2.y;
                         }
-                        // floor / fraction with packed arithmetic: pv >= 0 here, and at 1.5*2^23
-                        // the float spacing is 1, so a round-toward-zero add of 1.5*2^23 leaves
-                        // floor(pv) in the low mantissa bits; subtracting it back is exact
-                        const float2 t = __fadd2_rz(pv, f2(12582912.0f));
-                        const int ia = __float_as_int(t.x) - 0x4B400000, ib = __float_as_int(t.y) - 0x4B400000;
-                        const float2 fv = __fadd2_rn(pv, neg2(__fadd2_rn(t, f2(-12582912.0f))));
-                        const uint32_t aa = colb + (uint32_t)ia * rowb, ab = colb + (uint32_t)ib * rowb;
-                        const float2 r0 = f2(lds<TP>(aa), lds<TP>(ab)), r0r = f2(lds<TP>(aa + ES), lds<TP>(ab + ES));
-                        const float2 r1 = f2(lds<TP>(aa + rowb), lds<TP>(ab + rowb));
-                        const float2 r1r = f2(lds<TP>(aa + rowb + ES), lds<TP>(ab + rowb + ES));
-                        const float2 smp = lerp2(lerp2(r0, r0r, fu2), lerp2(r1, r1r, fu2), fv);
-                        float2 w = w2;
-                        if (MATCHED) {
-                            // w = L^3 / (DSD lsq); 1/sqrt(L^2) and 1/(DSD lsq) change by ~1e-4 relative per
-                            // slice, so one Newton-Raphson step from the previous pair's values
-                            // (y <- y (3 - x y^2)/2 ;  r <- r (2 - d r)) is accurate to ~1e-8
-                            const float2 vtex = __ffma2_rn(kk, vstep2, vt02);
-                            const float2 dz = __ffma2_rn(vtex, ddv2, dzc2);
-                            const float2 L2 = __ffma2_rn(dz, dz, cu22);
-                            const float2 rvz = __ffma2_rn(kk, dvz2, rz2);
-                            const float2 den = __fmul2_rn(__ffma2_rn(rvz, rvz, cxy2), dsd2);
-                            const float2 hl = __fmul2_rn(L2, f2(-0.5f));
-                            ys = __fmul2_rn(ys, __ffma2_rn(hl, __fmul2_rn(ys, ys), f2(1.5f)));
-                            rs = __fmul2_rn(rs, __ffma2_rn(neg2(den), rs, f2(2.0f)));
-                            w = __fmul2_rn(__fmul2_rn(L2, L2), __fmul2_rn(ys, rs));
-                        }
-                        const float2 acc2 = __ffma2_rn(smp, w, f2(acc[k], acc[k + 1]));
-                        acc[k] = acc2.x;
-                        acc[k + 1] = acc2.y;
-                    }
+                    };
+                    if (inside) pairs(std::false_type{});
+                    else pairs(std::true_type{});
                 } else {
                     // unrolled: a runtime index into acc[] would move it to local memory
 #pragma unroll
@@ -420,7 +433,8 @@ int launch_backproject_tma(TigrePlan* P, const void* proj, int pitch, int pdt, v
     CUtensorMap tm;
     cuuint64_t dims[3] = {(cuuint64_t)pitch, (cuuint64_t)P->d.nV, (cuuint64_t)na};
     cuuint64_t strides[2] = {(cuuint64_t)pitch * es, (cuuint64_t)pitch * P->d.nV * es};
-    cuuint32_t box[3] = {(cuuint32_t)P->bp_box_u, (cuuint32_t)P->bp_box_v, 1};
+    const int BU = pdt == TIGRE_F32 ? P->bp_box_u : P->bp_box_u16;
+    cuuint32_t box[3] = {(cuuint32_t)BU, (cuuint32_t)P->bp_box_v, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = enc(&tm, pdt == TIGRE_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3,
                      const_cast<void*>(proj), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -435,7 +449,7 @@ int launch_backproject_tma(TigrePlan* P, const void* proj, int pitch, int pdt, v
     a.na = na;
     a.nX = P->d.nX; a.nY = P->d.nY; a.nZ = P->d.nZ; a.nU = P->d.nU; a.nV = P->d.nV;
     a.pitch = pitch;
-    a.BU = P->bp_box_u;
+    a.BU = BU;
     a.BV = P->bp_box_v;
     a.dVZ = (float)P->d.dVZ;
     a.scale = matched ? (float)(P->d.dVX * P->d.dVY * P->d.dVZ / (P->d.dDU * P->d.dDV)) : 1.f;

@@ -279,7 +279,7 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
     // ---- staged backprojector constants and patch box ----
     plan->h_bpk.resize(nangles);
     double ext_u = 0.0, ext_v = 0.0;
-    const int bx = 16, bz = 16;
+    const int bx = kBpTile, bz = kBpSlices;
     for (int i = 0; i < nangles; ++i) {
         const FrameBP& f = plan->h_bp[i];
         FrameBPK& k = plan->h_bpk[i];
@@ -336,18 +336,28 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
                 }
     }
     {
-        int BU = ((int)std::ceil(ext_u) + 13 + 7) / 8 * 8;
-        while (BU % 32 != 8) BU += 8;   // row pitch = 8 banks mod 32: neighbouring rows do not collide
+        // Row pitch of the patch in 4-byte banks: = 4 (mod 8), so 8 neighbouring rows start in
+        // 8 distinct bank quads and the 4 taps of up to 8 rows x 4 columns per warp load do not
+        // collide.  The TMA box's row must be a multiple of 16 bytes: 4 floats, 8 halves.
+        const int need = (int)std::ceil(ext_u) + 13;
+        int BU = (std::max(need, 4) + 3) / 4 * 4;
+        while (BU % 8 != 4) BU += 4;                  // float rows: BU words
+        int BU16 = (std::max(need, 8) + 7) / 8 * 8;
+        while (BU16 % 16 != 8) BU16 += 8;             // 16-bit rows: BU16 / 2 words
         int BV = (int)std::ceil(ext_v) + 6;
-        if (BU < 8) BU = 8;
         if (BV < 4) BV = 4;
         if (const char* ov = std::getenv("TIGRE_B200_BP_BOX")) {   // test hook: force a box (e.g. "8x4")
             int bu = 0, bv = 0;
-            if (std::sscanf(ov, "%dx%d", &bu, &bv) == 2 && bu > 0 && bv > 0) { BU = (bu + 7) / 8 * 8; BV = bv; }
+            if (std::sscanf(ov, "%dx%d", &bu, &bv) == 2 && bu > 0 && bv > 0) {
+                BU = (bu + 3) / 4 * 4;
+                BU16 = (bu + 7) / 8 * 8;
+                BV = bv;
+            }
         }
-        const bool ok = std::isfinite(ext_u) && std::isfinite(ext_v) && BU <= 256 && BV <= 256 &&
+        const bool ok = std::isfinite(ext_u) && std::isfinite(ext_v) && BU16 <= 256 && BV <= 256 &&
                         2.0 * BU * BV * 4 <= 96.0 * 1024 && std::getenv("TIGRE_B200_NO_TMA") == nullptr;
         plan->bp_box_u = ok ? BU : 0;
+        plan->bp_box_u16 = ok ? BU16 : 0;
         plan->bp_box_v = ok ? BV : 0;
     }
     return TIGRE_SUCCESS;

@@ -124,6 +124,7 @@ struct TigrePlan {
     std::vector<tigre::FrameBPK> h_bpk;
     tigre::FrameBPK* d_bpk = nullptr;
     int bp_box_u = 0, bp_box_v = 0;   // TMA patch box of the staged backprojector (0: not usable)
+    int bp_box_u16 = 0;               // box width for 16-bit projections
     int* d_status = nullptr;          // kernel error word (bounded waits that expired)
     // growable stream-ordered scratch arena
     void* scratch = nullptr;
@@ -131,6 +132,10 @@ struct TigrePlan {
 };
 
 namespace tigre {
+
+// staged backprojector tiling: a block is kBpTile x kBpTile voxel columns of kBpSlices slices
+constexpr int kBpTile = 16;
+constexpr int kBpSlices = 32;
 
 int compute_frames(const TigreGeometry* geo, const float* angles, int nangles, TigrePlan* plan);
 void* plan_scratch(TigrePlan* plan, size_t bytes, cudaStream_t st, int* rc);
