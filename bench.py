@@ -182,6 +182,16 @@ def run_reference(args, rank):
         "cpu_baseline": {"kind": "reference", "cores": os.cpu_count(), "value": round(v, 4), "unit": "GRays/s",
                          "sample": "full workload; the reference has no CPU projector, its CUDA build runs on the GPU"},
     }
+    if not args.no_ops:
+        # the reference's other projector kinds through the same host API (one untimed call first)
+        ops = {}
+        _, t_int = ref.ax(img, geo, ang, "interpolated", repeat=2)
+        ops["ax_interpolated_f32"] = {"value": round(rays / t_int[-1] / 1e9, 4), "unit": "GRays/s",
+                                      "ms_per_call": round(1e3 * t_int[-1], 3)}
+        _, t_fdk = ref.atb(proj, geo, ang, "FDK", repeat=2)
+        ops["atb_fdk_f32"] = {"value": round(upd / t_fdk[-1] / 1e9, 4), "unit": "Gvox-upd/s",
+                              "ms_per_call": round(1e3 * t_fdk[-1], 3)}
+        line["ops"] = ops
     print(json.dumps(line))
 
 

@@ -82,14 +82,28 @@ int tigre_ax(TigrePlan* plan, const void* d_vol, int vdt, void* d_proj, int pdt,
         return launch_siddon(plan, vx, vy, vdt, d_proj, pdt, a0, a1, st);
     }
     if (projector == TIGRE_PROJ_INTERPOLATED) {
-        const size_t padded = (size_t)(d.nX + 3) * (d.nY + 3) * (d.nZ + 3) * es;
-        char* s = (char*)plan_scratch(plan, padded * 2, st, &rc);
+        // zero-padded copies (1 before, 2 after), x- and/or y-fastest; trilinear sampling reads
+        // corner quads built from them (4 values per element), point sampling the copies
+        // (offsets rounded to 256 bytes: the quads are read as 8- or 16-byte vectors)
+        const size_t padded = ((size_t)(d.nX + 3) * (d.nY + 3) * (d.nZ + 3) * es + 255) / 256 * 256;
+        const bool nearest = d.accuracy > 1.0;
+        char* s = (char*)plan_scratch(plan, padded * (nearest ? 2 : 9), st, &rc);
         if (rc) return rc;
         void* vx = s;
         void* vy = s + padded;
-        if (l0 && (rc = launch_make_layout(d_vol, vdt, vx, d.nX, d.nY, d.nZ, 0, 1, 2, st))) return rc;
-        if (l1 && (rc = launch_make_layout(d_vol, vdt, vy, d.nX, d.nY, d.nZ, 1, 1, 2, st))) return rc;
-        return launch_interp(plan, vx, vy, vdt, d_proj, pdt, a0, a1, st);
+        void* qx = nearest ? nullptr : s + padded;
+        void* qy = nearest ? nullptr : s + 5 * padded;
+        if (nearest) {
+            if (l0 && (rc = launch_make_layout(d_vol, vdt, vx, d.nX, d.nY, d.nZ, 0, 1, 2, st))) return rc;
+            if (l1 && (rc = launch_make_layout(d_vol, vdt, vy, d.nX, d.nY, d.nZ, 1, 1, 2, st))) return rc;
+        } else {
+            for (int l = 0; l < 2; ++l) {
+                if (!(l ? l1 : l0)) continue;
+                if ((rc = launch_make_layout(d_vol, vdt, vx, d.nX, d.nY, d.nZ, l, 1, 2, st))) return rc;
+                if ((rc = launch_make_quads(vx, vdt, l ? qy : qx, d.nX, d.nY, d.nZ, l, st))) return rc;
+            }
+        }
+        return launch_interp(plan, vx, vy, qx, qy, vdt, d_proj, pdt, a0, a1, st);
     }
     return fail(TIGRE_ERR_BAD_ASSERT, "unknown projector");
 }

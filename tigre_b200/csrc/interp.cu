@@ -18,6 +18,7 @@
 //    after, per axis), x- or y-fastest per view like the Siddon kernel, so the
 //    8-corner gather needs no bounds tests.
 
+#include <climits>
 #include <cmath>
 
 #include "tigre_internal.h"
@@ -26,8 +27,10 @@ namespace tigre {
 namespace {
 
 struct InterpArgs {
-    const void* vol_x;   // padded, (nZ+3, nY+3, nX+3)
+    const void* vol_x;   // padded, (nZ+3, nY+3, nX+3)       (point sampling)
     const void* vol_y;   // padded, (nZ+3, nX+3, nY+3)
+    const void* quad_x;  // corner quads of vol_x / vol_y   (trilinear sampling)
+    const void* quad_y;
     void* proj;
     const FrameInterp* frames;
     int a0;
@@ -35,12 +38,45 @@ struct InterpArgs {
     double dVX, dVY, dVZ, acc;
 };
 
+// one corner quad (fast axis x z 2x2 block) as floats
+template <typename TV> __device__ __forceinline__ float4 ldq(const void* base, uint32_t i);
+template <> __device__ __forceinline__ float4 ldq<float>(const void* base, uint32_t i) {
+    return __ldg(reinterpret_cast<const float4*>(base) + i);
+}
+template <> __device__ __forceinline__ float4 ldq<__nv_bfloat16>(const void* base, uint32_t i) {
+    const uint2 r = __ldg(reinterpret_cast<const uint2*>(base) + i);
+    return make_float4(__uint_as_float(r.x << 16), __uint_as_float(r.x & 0xffff0000u), __uint_as_float(r.y << 16),
+                       __uint_as_float(r.y & 0xffff0000u));
+}
+template <> __device__ __forceinline__ float4 ldq<__half>(const void* base, uint32_t i) {
+    const uint2 r = __ldg(reinterpret_cast<const uint2*>(base) + i);
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&r.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&r.y));
+    return make_float4(a.x, a.y, b.x, b.y);
+}
+
+// trilinear value from the quads of rows o and o+1 (fractions along fast, z, other)
+__device__ __forceinline__ float tri(const float4 q0, const float4 q1, float ff, float fz, float fo) {
+    const float a0 = fmaf(ff, q0.y - q0.x, q0.x), a1 = fmaf(ff, q0.w - q0.z, q0.z);
+    const float b0 = fmaf(ff, q1.y - q1.x, q1.x), b1 = fmaf(ff, q1.w - q1.z, q1.z);
+    const float r0 = fmaf(fz, a1 - a0, a0), r1 = fmaf(fz, b1 - b0, b0);
+    return fmaf(fo, r1 - r0, r0);
+}
+
+__device__ __forceinline__ float2 pk2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 pk2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 t) {
+    return __ffma2_rn(t, __ffma2_rn(a, pk2(-1.f), b), a);
+}
+
 template <typename TV, typename TP, bool NEAREST>
 __global__ void __launch_bounds__(256) interp_kernel(InterpArgs p) {
-    const int u = blockIdx.x * 32 + threadIdx.x;
+    const int u0 = blockIdx.x * 32 + threadIdx.x;
     const int v = blockIdx.y * blockDim.y + threadIdx.y;
     const int la = blockIdx.z;
-    if (u >= p.nU || v >= p.nV) return;
+    if (v >= p.nV) return;   // a warp is one detector row: uniform
+    const bool in_u = u0 < p.nU;
+    const int u = in_u ? u0 : p.nU - 1;
     const FrameInterp& F = p.frames[p.a0 + la];
     const double pv = (double)(p.nV - 1 - v);
     double d[3], s[3];
@@ -66,16 +102,25 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs p) {
             empty = true;
         }
     }
+    const bool live = in_u && !empty && lo <= hi;
+    // The lanes of a warp walk one global sample index i from the warp's smallest first
+    // sample: at each step their samples sit at the same fraction of neighbouring rays, so
+    // the warp's gathers stay compact.  A lane's samples before its own first one lie outside
+    // the volume (beyond the first-sample cap of the view they are not taken at all, and lo
+    // is never below it), clamp to the zero pads and add nothing.
+    const int i0 = __reduce_min_sync(0xffffffffu, live ? (int)lo : INT_MAX);
+    if (!in_u) return;
     const size_t oidx = ((size_t)la * p.nV + v) * (size_t)p.nU + u;
-    if (empty || lo > hi) {
+    if (!live) {
         ((TP*)p.proj)[oidx] = from_f32<TP>(0.f);
         return;
     }
-    const int nsamp = (int)(hi - lo) + 1;
+    const int first = NEAREST ? (int)lo : i0;
+    const int nsamp = (int)hi - first + 1;
     // padded coordinates (+1) of the first sample
-    const float q0x = (float)(fma(vec[0], lo, s[0]) + 1.0);
-    const float q0y = (float)(fma(vec[1], lo, s[1]) + 1.0);
-    const float q0z = (float)(fma(vec[2], lo, s[2]) + 1.0);
+    const float q0x = (float)(fma(vec[0], (double)first, s[0]) + 1.0);
+    const float q0y = (float)(fma(vec[1], (double)first, s[1]) + 1.0);
+    const float q0z = (float)(fma(vec[2], (double)first, s[2]) + 1.0);
     const float vx = (float)vec[0], vy = (float)vec[1], vz = (float)vec[2];
     const float mx = (float)(p.nX + 1), my = (float)(p.nY + 1), mz = (float)(p.nZ + 1);
     const int XP = p.nX + 3, YP = p.nY + 3;
@@ -85,27 +130,62 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs p) {
     const int sy = layout ? 1 : XP;
     const int sz = XP * YP;
     float sum = 0.f;
+    if (NEAREST) {
 #pragma unroll 2
-    for (int k = 0; k < nsamp; ++k) {
-        const float kf = (float)k;
-        const float qx = fminf(fmaxf(fmaf(kf, vx, q0x), 0.f), mx);
-        const float qy = fminf(fmaxf(fmaf(kf, vy, q0y), 0.f), my);
-        const float qz = fminf(fmaxf(fmaf(kf, vz, q0z), 0.f), mz);
-        if (NEAREST) {
+        for (int k = 0; k < nsamp; ++k) {
+            const float kf = (float)k;
+            const float qx = fminf(fmaxf(fmaf(kf, vx, q0x), 0.f), mx);
+            const float qy = fminf(fmaxf(fmaf(kf, vy, q0y), 0.f), my);
+            const float qz = fminf(fmaxf(fmaf(kf, vz, q0z), 0.f), mz);
             const int ix = (int)(qx + 0.5f), iy = (int)(qy + 0.5f), iz = (int)(qz + 0.5f);
             sum += ldg_f<TV>(vol + ix * sx + iy * sy + iz * sz);
-        } else {
-            const int ix = (int)qx, iy = (int)qy, iz = (int)qz;
-            const float fx = qx - (float)ix, fy = qy - (float)iy, fz = qz - (float)iz;
-            const TV* b = vol + ix * sx + iy * sy + iz * sz;
-            const float c000 = ldg_f<TV>(b), c100 = ldg_f<TV>(b + sx);
-            const float c010 = ldg_f<TV>(b + sy), c110 = ldg_f<TV>(b + sx + sy);
-            const float c001 = ldg_f<TV>(b + sz), c101 = ldg_f<TV>(b + sx + sz);
-            const float c011 = ldg_f<TV>(b + sy + sz), c111 = ldg_f<TV>(b + sx + sy + sz);
-            const float c00 = fmaf(fx, c100 - c000, c000), c10 = fmaf(fx, c110 - c010, c010);
-            const float c01 = fmaf(fx, c101 - c001, c001), c11 = fmaf(fx, c111 - c011, c011);
-            const float c0 = fmaf(fy, c10 - c00, c00), c1 = fmaf(fy, c11 - c01, c01);
-            sum += fmaf(fz, c1 - c0, c0);
+        }
+    } else {
+        // Trilinear from corner quads: with f the fast axis of this view's layout and o the
+        // other one, a sample is two vector loads (rows o and o+1).  Two samples per step in
+        // packed FP32x2.  Floors by a round-toward-zero add of 1.5*2^23 (the clamped
+        // coordinates are >= 0); the float bits then index the quads directly:
+        // index = bf + bo*FP + bz*FP*OP - 0x4B400000*(1 + FP + FP*OP) (32-bit wrap).
+        constexpr float M = 12582912.0f;
+        const float q0f = layout ? q0y : q0x, q0o = layout ? q0x : q0y;
+        const float vf = layout ? vy : vx, vo = layout ? vx : vy;
+        const float mf = layout ? my : mx, mo = layout ? mx : my;
+        const uint32_t FP = (uint32_t)(layout ? YP : XP), OP = (uint32_t)(layout ? XP : YP);
+        const uint32_t PL = FP * OP;
+        const uint32_t bias = 0u - 0x4B400000u * (1u + FP + PL);
+        const void* quads = layout ? p.quad_y : p.quad_x;
+        const float2 vf2 = pk2(vf), vo2 = pk2(vo), vz2 = pk2(vz);
+        const float2 q0f2 = pk2(q0f), q0o2 = pk2(q0o), q0z2 = pk2(q0z);
+        float2 kk = pk2(0.f, 1.f);
+        float sa = 0.f, sb = 0.f;
+        int k = 0;
+#pragma unroll 1
+        for (; k + 1 < nsamp; k += 2) {
+            float2 qf = __ffma2_rn(kk, vf2, q0f2), qo = __ffma2_rn(kk, vo2, q0o2), qz = __ffma2_rn(kk, vz2, q0z2);
+            kk = __fadd2_rn(kk, pk2(2.f));
+            qf.x = fminf(fmaxf(qf.x, 0.f), mf); qf.y = fminf(fmaxf(qf.y, 0.f), mf);
+            qo.x = fminf(fmaxf(qo.x, 0.f), mo); qo.y = fminf(fmaxf(qo.y, 0.f), mo);
+            qz.x = fminf(fmaxf(qz.x, 0.f), mz); qz.y = fminf(fmaxf(qz.y, 0.f), mz);
+            const float2 tf = __fadd2_rz(qf, pk2(M)), to = __fadd2_rz(qo, pk2(M)), tz = __fadd2_rz(qz, pk2(M));
+            const float2 ff = __ffma2_rn(__fadd2_rn(tf, pk2(-M)), pk2(-1.f), qf);
+            const float2 fo = __ffma2_rn(__fadd2_rn(to, pk2(-M)), pk2(-1.f), qo);
+            const float2 fz = __ffma2_rn(__fadd2_rn(tz, pk2(-M)), pk2(-1.f), qz);
+            const uint32_t ia = __float_as_uint(tf.x) + __float_as_uint(to.x) * FP + __float_as_uint(tz.x) * PL + bias;
+            const uint32_t ib = __float_as_uint(tf.y) + __float_as_uint(to.y) * FP + __float_as_uint(tz.y) * PL + bias;
+            const float4 a0 = ldq<TV>(quads, ia), a1 = ldq<TV>(quads, ia + FP);
+            const float4 b0 = ldq<TV>(quads, ib), b1 = ldq<TV>(quads, ib + FP);
+            sa += tri(a0, a1, ff.x, fz.x, fo.x);
+            sb += tri(b0, b1, ff.y, fz.y, fo.y);
+        }
+        sum = sa + sb;
+        if (k < nsamp) {   // odd count: last sample
+            const float kf = (float)k;
+            const float qf = fminf(fmaxf(fmaf(kf, vf, q0f), 0.f), mf);
+            const float qo = fminf(fmaxf(fmaf(kf, vo, q0o), 0.f), mo);
+            const float qz = fminf(fmaxf(fmaf(kf, vz, q0z), 0.f), mz);
+            const float tf = __fadd_rz(qf, M), to = __fadd_rz(qo, M), tz = __fadd_rz(qz, M);
+            const uint32_t i = __float_as_uint(tf) + __float_as_uint(to) * FP + __float_as_uint(tz) * PL + bias;
+            sum += tri(ldq<TV>(quads, i), ldq<TV>(quads, i + FP), qf - (tf - M), qz - (tz - M), qo - (to - M));
         }
     }
     const double dl = sqrt(vec[0] * p.dVX * vec[0] * p.dVX + vec[1] * p.dVY * vec[1] * p.dVY +
@@ -121,10 +201,10 @@ void launch_typed(const InterpArgs& a, bool nearest, dim3 grid, dim3 block, cuda
 
 }  // namespace
 
-int launch_interp(TigrePlan* P, const void* vol_x, const void* vol_y, int vdt, void* proj, int pdt, int a0, int a1,
-                  cudaStream_t st) {
+int launch_interp(TigrePlan* P, const void* vol_x, const void* vol_y, const void* quad_x, const void* quad_y, int vdt,
+                  void* proj, int pdt, int a0, int a1, cudaStream_t st) {
     InterpArgs a{};
-    a.vol_x = vol_x; a.vol_y = vol_y; a.frames = P->d_interp;
+    a.vol_x = vol_x; a.vol_y = vol_y; a.quad_x = quad_x; a.quad_y = quad_y; a.frames = P->d_interp;
     a.nX = P->d.nX; a.nY = P->d.nY; a.nZ = P->d.nZ; a.nU = P->d.nU; a.nV = P->d.nV;
     a.dVX = P->d.dVX; a.dVY = P->d.dVY; a.dVZ = P->d.dVZ; a.acc = P->d.accuracy;
     const bool nearest = P->d.accuracy > 1.0;

@@ -73,6 +73,30 @@ __global__ void make_zfast_kernel(const T* __restrict__ src, T* __restrict__ dst
     }
 }
 
+// Corner quads for the interpolated projector: from a padded copy (layout 0: x fastest,
+// layout 1: y fastest; F = padded fast extent, O = padded other extent, Z = padded z extent),
+// element i = (p[i], p[i+1], p[i+F*O], p[i+1+F*O]) -- the fast-axis x z 2x2 corner block of
+// a trilinear sample, read as one vector load.  Corners past the last fast or z index are 0
+// (no sample has its base there).
+template <typename T>
+struct Quad4 { T v[4]; };
+
+template <typename T>
+__global__ void make_quads_kernel(const T* __restrict__ pad, Quad4<T>* __restrict__ dst, int F, int O, int Z) {
+    const long plane = (long)F * O, total = plane * Z;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int f = (int)(i % F);
+        const long zp = i / plane;
+        const bool f1 = f + 1 < F, z1 = zp + 1 < Z;
+        Quad4<T> q;
+        q.v[0] = pad[i];
+        q.v[1] = f1 ? pad[i + 1] : from_f32<T>(0.f);
+        q.v[2] = z1 ? pad[i + plane] : from_f32<T>(0.f);
+        q.v[3] = (f1 && z1) ? pad[i + plane + 1] : from_f32<T>(0.f);
+        dst[i] = q;
+    }
+}
+
 template <typename T>
 __global__ void pad_projections_kernel(const T* __restrict__ src, T* __restrict__ dst, int nV, int nU, long total) {
     const long pitch = bp_pitch(nU), rows = bp_rows(nV);
@@ -129,6 +153,17 @@ int launch_make_zfast(const void* src, int dtype, void* dst, int nX, int nY, int
     dim3 grid((nZ + 2 * zpad + TILE - 1) / TILE, (nX + TILE - 1) / TILE, nY);
     TIGRE_DISPATCH_DTYPE(dtype, T, {
         make_zfast_kernel<T><<<grid, block, 0, st>>>((const T*)src, (T*)dst, nX, nY, nZ, zpad);
+    });
+    TIGRE_LAUNCHED();
+    return TIGRE_SUCCESS;
+}
+
+int launch_make_quads(const void* pad, int dtype, void* dst, int nX, int nY, int nZ, int layout, cudaStream_t st) {
+    const int F = (layout ? nY : nX) + 3, O = (layout ? nX : nY) + 3, Z = nZ + 3;
+    const long total = (long)F * O * Z;
+    const int grid = (int)std::min<long>((total + 255) / 256, 148L * 32);
+    TIGRE_DISPATCH_DTYPE(dtype, T, {
+        make_quads_kernel<T><<<grid, 256, 0, st>>>((const T*)pad, (Quad4<T>*)dst, F, O, Z);
     });
     TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;

@@ -144,6 +144,7 @@ void* plan_scratch(TigrePlan* plan, size_t bytes, cudaStream_t st, int* rc);
 int launch_make_layout(const void* src, int dtype, void* dst, int nX, int nY, int nZ, int layout, int pad_lo,
                        int pad_hi, cudaStream_t st);
 int launch_pad_projections(const void* src, int dtype, void* dst, int nA, int nV, int nU, cudaStream_t st);
+int launch_make_quads(const void* pad, int dtype, void* dst, int nX, int nY, int nZ, int layout, cudaStream_t st);
 int launch_make_zfast(const void* src, int dtype, void* dst, int nX, int nY, int nZ, int zpad, cudaStream_t st);
 
 int launch_siddon(TigrePlan* p, const void* vol_x, const void* vol_y, int vdt, void* proj, int pdt, int a0, int a1,
@@ -153,8 +154,8 @@ int launch_siddon_cells(TigrePlan* p, const void* vol_z, int vdt, void* proj, in
                         cudaStream_t st);
 int launch_siddon_columns(TigrePlan* p, const void* vol_z, int vdt, void* proj, int pdt, int a0, int a1,
                           cudaStream_t st);
-int launch_interp(TigrePlan* p, const void* vol_x, const void* vol_y, int vdt, void* proj, int pdt, int a0, int a1,
-                  cudaStream_t st);
+int launch_interp(TigrePlan* p, const void* vol_x, const void* vol_y, const void* quad_x, const void* quad_y, int vdt,
+                  void* proj, int pdt, int a0, int a1, cudaStream_t st);
 int launch_backproject(TigrePlan* p, const void* proj_pad, int pdt, void* vol, int vdt, int matched, int a0, int a1,
                        int accumulate, cudaStream_t st);
 
