@@ -152,6 +152,19 @@ def _phantom_host(seed):
     return _PH[seed]
 
 
+def max_over_ranks(dist, values, device):
+    """Element-wise maximum of per-rank device times (the slowest rank sets the job time)."""
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def job_throughput(world, units_per_rank, seconds):
+    """Whole-job rate in G units/s: every replica processes units_per_rank in the max-over-ranks time."""
+    return world * units_per_rank / seconds / 1e9
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -257,13 +270,11 @@ def main():
     t_atb = sum(e[1].elapsed_time(e[2]) for e in ev) / 1e3
     t_tot = ev[0][0].elapsed_time(ev[-1][2]) / 1e3
     if dist:
-        t = torch.tensor([t_ax, t_atb, t_tot], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ax, t_atb, t_tot = t.tolist()
+        t_ax, t_atb, t_tot = max_over_ranks(dist, [t_ax, t_atb, t_tot], dev)
     rays = NA * NU * NV
     upd = NA * math.prod(NVOX)
-    value = world * rays * args.steps / t_ax / 1e9
-    atb_value = world * upd * args.steps / t_atb / 1e9
+    value = job_throughput(world, rays * args.steps, t_ax)
+    atb_value = job_throughput(world, upd * args.steps, t_atb)
     # roofline of the dominant kernel, algorithmic bytes per launch
     peak, peak_kind = peaks()
     ax_launch = t_ax / args.steps
@@ -320,12 +331,12 @@ def main():
         dist.destroy_process_group()
 
 
-# DRAM bytes per launch per view, from ncu captures of the 512^3 workload at 36 views
-# (dram__bytes_read.sum + dram__bytes_write.sum; profiles/siddon_columns_512cube_36views.txt and
-# profiles/bp_tma_matched_512cube_36views.txt), scaled to the timed launch by its view count.
-# Traffic grows with the views processed: the volume is re-read per view group, the projections
-# are read or written once.
-TRAFFIC_PER_VIEW = {"siddon": None, "bp": None}
+# DRAM bytes per view of the Siddon launch on the 512^3 workload, from an ncu capture of 36 views
+# (dram__bytes_read.sum + dram__bytes_write.sum = 9.991 GB; profiles/siddon_cells_512cube_36views.txt),
+# scaled to the timed launch by its view count: each view re-reads the part of the volume it crosses
+# and writes its projection once.  The backprojector's DRAM traffic is one volume write plus one
+# read of the projections, not proportional to the views, so it is not scaled.
+TRAFFIC_PER_VIEW = {"siddon": 277525119, "bp": None}
 
 
 def _scaled_traffic(kind, views):
