@@ -381,7 +381,7 @@ __device__ __forceinline__ float ldz(uintptr_t cb, float t) {
 }
 
 template <typename TV, typename TP, int R>
-__global__ void __launch_bounds__(128, 5) siddon_cells_kernel(SiddonArgs p) {
+__global__ void __launch_bounds__(128, 6) siddon_cells_kernel(SiddonArgs p) {
     static_assert(R % 2 == 0, "rows are processed in pairs");
     constexpr int H = R / 2;
     const int lane = threadIdx.x & 31;
