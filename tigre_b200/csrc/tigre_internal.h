@@ -135,7 +135,7 @@ namespace tigre {
 
 // staged backprojector tiling: a block is kBpTile x kBpTile voxel columns of kBpSlices slices
 constexpr int kBpTile = 16;
-constexpr int kBpSlices = 32;
+constexpr int kBpSlices = 64;
 
 int compute_frames(const TigreGeometry* geo, const float* angles, int nangles, TigrePlan* plan);
 void* plan_scratch(TigrePlan* plan, size_t bytes, cudaStream_t st, int* rc);
