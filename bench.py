@@ -332,11 +332,11 @@ def main():
 
 
 # DRAM bytes per view of the Siddon launch on the 512^3 workload, from an ncu capture of 36 views
-# (dram__bytes_read.sum + dram__bytes_write.sum = 9.991 GB; profiles/siddon_cells_512cube_36views.txt),
+# (dram__bytes_read.sum + dram__bytes_write.sum = 10.337 GB; profiles/siddon_cells_512cube_36views.txt),
 # scaled to the timed launch by its view count: each view re-reads the part of the volume it crosses
 # and writes its projection once.  The backprojector's DRAM traffic is one volume write plus one
 # read of the projections, not proportional to the views, so it is not scaled.
-TRAFFIC_PER_VIEW = {"siddon": 277525119, "bp": None}
+TRAFFIC_PER_VIEW = {"siddon": 287152417, "bp": None}
 
 
 def _scaled_traffic(kind, views):
