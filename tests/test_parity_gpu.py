@@ -300,3 +300,54 @@ print('ok')
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env,
                        cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))), timeout=600)
     assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
+
+
+@pytest.mark.parametrize("dt", ["bfloat16", "float16"])
+def test_reduced_storage_equals_fp32_on_rounded_inputs(dt):
+    """BF16 / FP16 storage changes only what is stored: each projector kind run on 16-bit
+    inputs (FP32 output) equals the FP32 path run on the same inputs rounded to 16 bits."""
+    torch = _torch()
+    from tigre_b200 import _native as N, projectors as P
+    tdt = getattr(torch, dt)
+    geo, ang = G.odd_geometry(), G.angles(17, full=np.pi * 1.3)
+    img = G.phantom(tuple(int(v) for v in geo.nVoxel), seed=9)
+    plan = N.get_plan(N.checked_geometry(geo, ang), 0)
+    v16 = torch.from_numpy(img).cuda().to(tdt)
+    v32 = v16.float()
+    for ptype in ("Siddon", "interpolated"):
+        got = P.ax(v16, plan, ptype, out_dtype=torch.float32).cpu().numpy()
+        ref = P.ax(v32, plan, ptype).cpu().numpy()
+        mx, l2 = G.rel_err(got, ref)
+        assert mx <= 1e-5 and l2 <= 1e-6, (dt, ptype, mx, l2)
+    p16 = torch.from_numpy(O.ax(img, geo, ang, "Siddon")).cuda().to(tdt)
+    p32 = p16.float()
+    for bt in ("FDK", "matched"):
+        got = P.atb(p16, plan, bt, out_dtype=torch.float32).cpu().numpy()
+        ref = P.atb(p32, plan, bt).cpu().numpy()
+        mx, l2 = G.rel_err(got, ref)
+        assert mx <= 1e-5 and l2 <= 1e-6, (dt, bt, mx, l2)
+    assert plan.status() == 0
+
+
+def test_interpolated_point_sampling_matches_oracle():
+    """accuracy > 1 switches the interpolated projector to point sampling (the reference's
+    texture switches to cudaFilterModePoint, ray_interpolated_projection.cu:589-592).
+
+    Point sampling is discontinuous where a sample crosses a voxel half-boundary: the sample
+    positions are FP32 here (as in the reference), FP64 in the oracle, so a sample within
+    ~1e-4 voxel of a boundary may pick the neighbouring voxel.  Such a ray differs by one
+    sample's value; every other ray must agree to the parity bar."""
+    torch = _torch()
+    from tigre_b200 import _native as N, projectors as P
+    geo, ang = G.c1_geometry(), G.angles(24)
+    geo.accuracy = 2.0
+    img = G.phantom((64, 64, 64), seed=6)
+    plan = N.get_plan(N.checked_geometry(geo, ang), 0)
+    got = P.ax(torch.from_numpy(img).cuda(), plan, "interpolated").cpu().numpy().astype(np.float64)
+    ref = O.ax(img, geo, ang, "interpolated").astype(np.float64)
+    err = np.abs(got - ref) / np.abs(ref).max()
+    bad = err > TOL
+    # one flipped sample changes a ray by at most (max voxel) x (sample length in mm)
+    one_sample = float(img.max()) * 2.0 * 1.0 / np.abs(ref).max()
+    assert bad.mean() <= 2e-3, (bad.mean(), err.max())
+    assert err.max() <= 2.0 * one_sample, (err.max(), one_sample)

@@ -71,9 +71,11 @@ __device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 t) {
 
 template <typename TV, typename TP, bool NEAREST>
 __global__ void __launch_bounds__(256) interp_kernel(InterpArgs p) {
+    // grid: detector column groups fastest, then views, then bands of detector rows, so the
+    // z-slab of the volume that one band of rows crosses stays L2-resident across all views
     const int u0 = blockIdx.x * 32 + threadIdx.x;
-    const int v = blockIdx.y * blockDim.y + threadIdx.y;
-    const int la = blockIdx.z;
+    const int la = blockIdx.y;
+    const int v = blockIdx.z * blockDim.y + threadIdx.y;
     if (v >= p.nV) return;   // a warp is one detector row: uniform
     const bool in_u = u0 < p.nU;
     const int u = in_u ? u0 : p.nU - 1;
@@ -210,13 +212,13 @@ int launch_interp(TigrePlan* P, const void* vol_x, const void* vol_y, const void
     const bool nearest = P->d.accuracy > 1.0;
     const int rows = 8;
     dim3 block(32, rows);
-    dim3 grid((P->d.nU + 31) / 32, (P->d.nV + rows - 1) / rows, 1);
+    dim3 grid((P->d.nU + 31) / 32, 1, (P->d.nV + rows - 1) / rows);
     const int na = a1 - a0;
     for (int c = 0; c < na; c += 65535) {
         InterpArgs ac = a;
         ac.a0 = a0 + c;
         ac.proj = (char*)proj + (size_t)c * P->d.nU * P->d.nV * dtype_size(pdt);
-        grid.z = std::min(65535, na - c);
+        grid.y = std::min(65535, na - c);
         if (vdt == TIGRE_F32 && pdt == TIGRE_F32) launch_typed<float, float>(ac, nearest, grid, block, st);
         else if (vdt == TIGRE_BF16 && pdt == TIGRE_BF16)
             launch_typed<__nv_bfloat16, __nv_bfloat16>(ac, nearest, grid, block, st);
