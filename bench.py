@@ -398,11 +398,21 @@ def measure_e2e(vol, geo, ang, steps):
         t = time.perf_counter()
         tigre.Atb(pin_np, geo, ang, "matched")
         tb.append(time.perf_counter() - t)
+    # the other two kinds through the same host API (one untimed call first, one timed)
+    tigre.Ax(img_np, geo, ang, "interpolated")
+    t = time.perf_counter()
+    tigre.Ax(img_np, geo, ang, "interpolated")
+    ti = time.perf_counter() - t
+    tigre.Atb(pin_np, geo, ang, "FDK")
+    t = time.perf_counter()
+    tigre.Atb(pin_np, geo, ang, "FDK")
+    tf = time.perf_counter() - t
     rays, upd = NA * NU * NV, NA * math.prod(NVOX)
     b_vol, b_proj = math.prod(NVOX) * 4, NA * NU * NV * 4
     return {"value": round(rays / statistics.median(ta) / 1e9, 4), "unit": "GRays/s",
             "atb_value": round(upd / statistics.median(tb) / 1e9, 4), "atb_unit": "Gvox-upd/s",
             "ax_s": round(statistics.median(ta), 4), "atb_s": round(statistics.median(tb), 4),
+            "interpolated_value": round(rays / ti / 1e9, 4), "fdk_value": round(upd / tf / 1e9, 4),
             "h2d_bytes_per_step": b_vol + b_proj, "d2h_bytes_per_step": b_proj + b_vol}
 
 

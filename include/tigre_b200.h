@@ -117,10 +117,12 @@ int tigre_voxel_backprojection2(const float* projections, const TigreGeometry* g
 int tigre_pocs_tv(const float* img, float* dst, float alpha, const long* image_size, int max_iter,
                   const int* gpu_ids, int n_gpus);
 
-/* Parallel-beam entry points referenced by the reference's Cython layer
- * (_Ax.pyx:21-26, _Atb.pyx:21-22: siddon_ray_projection_parallel,
- * interpolation_projection_parallel, voxel_backprojection_parallel).  Parallel
- * beam is outside this library: they return TIGRE_ERR_BAD_ASSERT. */
+/* Parallel-beam projection and backprojection.  Replace siddon_ray_projection_parallel
+ * (Common/CUDA/Siddon_projection_parallel.hpp, Siddon_projection_parallel.cu:270),
+ * interpolation_projection_parallel (ray_interpolated_projection_parallel.hpp,
+ * ray_interpolated_projection_parallel.cu:195) and voxel_backprojection_parallel
+ * (voxel_backprojection_parallel.hpp, voxel_backprojection_parallel.cu), called by
+ * _Ax.pyx:85-87 and _Atb.pyx:75.  Same arguments as the cone-beam calls. */
 int tigre_siddon_ray_projection_parallel(const float* img, const TigreGeometry* geo, float* const* result,
                                          const float* angles, int nangles, const int* gpu_ids, int n_gpus);
 int tigre_interpolation_projection_parallel(const float* img, const TigreGeometry* geo, float* const* result,
@@ -138,6 +140,12 @@ int tigre_voxel_backprojection_parallel(const float* projections, const TigreGeo
 typedef struct TigrePlan TigrePlan;
 
 int tigre_plan_create(const TigreGeometry* geo, const float* angles, int nangles, int device, TigrePlan** plan);
+/* As tigre_plan_create; flags: TIGRE_PLAN_PARALLEL for a parallel-beam geometry (the frames
+ * of the reference's *_parallel functions; tigre_ax / tigre_atb then project and backproject
+ * in parallel beam, and the backprojector type is ignored, as in the reference). */
+#define TIGRE_PLAN_PARALLEL 1
+int tigre_plan_create_ex(const TigreGeometry* geo, const float* angles, int nangles, int device, int flags,
+                         TigrePlan** plan);
 void tigre_plan_destroy(TigrePlan* plan);
 /* Bytes of device scratch currently held by the plan. */
 long long tigre_plan_scratch_bytes(const TigrePlan* plan);

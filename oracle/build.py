@@ -27,9 +27,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # the reference's own extension groupings (setup.py:347-433)
 REF_GROUPS = {
     "ax": (["projection.cpp", "TIGRE_common.cpp", "GpuIds.cpp", "Siddon_projection.cu",
-            "ray_interpolated_projection.cu"], "REF_AX"),
+            "Siddon_projection_parallel.cu", "ray_interpolated_projection.cu",
+            "ray_interpolated_projection_parallel.cu"], "REF_AX"),
     "atb": (["TIGRE_common.cpp", "GpuIds.cpp", "gpuUtils.cu", "voxel_backprojection.cu",
-             "voxel_backprojection2.cu"], "REF_ATB"),
+             "voxel_backprojection2.cu", "voxel_backprojection_parallel.cu"], "REF_ATB"),
     "tv": (["TIGRE_common.cpp", "GpuIds.cpp", "gpuUtils.cu", "GD_TV.cu"], "REF_TV"),
 }
 

@@ -56,6 +56,10 @@ def lib():
         _LIB.oracle_interp.argtypes = [f, C.POINTER(OGeo), C.c_int, C.c_int, C.c_int, C.c_int, f, f, C.c_int]
         _LIB.oracle_backproject.argtypes = [f, C.POINTER(OGeo), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, f,
                                             C.c_int]
+        _LIB.oracle_siddon_parallel.argtypes = [f, C.POINTER(OGeo), C.c_int, C.c_int, C.c_int, C.c_int, f, C.c_int]
+        _LIB.oracle_interp_parallel.argtypes = [f, C.POINTER(OGeo), C.c_int, C.c_int, C.c_int, C.c_int, f, C.c_int]
+        _LIB.oracle_backproject_parallel.argtypes = [f, C.POINTER(OGeo), C.c_int, C.c_int, C.c_int, C.c_int, f,
+                                                     C.c_int]
         _LIB.oracle_tv_gradient.argtypes = [f, C.c_long, C.c_long, C.c_long, f, C.c_int]
         _LIB.oracle_pocs_tv.argtypes = [f, f, C.c_float, C.c_long, C.c_long, C.c_long, C.c_int, C.c_int]
     return _LIB
@@ -120,8 +124,14 @@ def ax(img, geo, angles, projection_type="Siddon", angle_range=None, row_range=N
     img = _f32(img)
     assert img.shape == (s.nVoxelZ, s.nVoxelY, s.nVoxelX)
     out = np.zeros((a1 - a0, v1 - v0, s.nDetecU), dtype=np.float32)
+    siddon = projection_type in ("Siddon", "ray-voxel")
+    if getattr(G.g, "mode", "cone") == "parallel":
+        assert not return_counts, "counts are kept for cone beam only"
+        fn = lib().oracle_siddon_parallel if siddon else lib().oracle_interp_parallel
+        fn(img.ctypes.data, C.byref(s), a0, a1, v0, v1, out.ctypes.data, _threads(nthreads))
+        return out
     cnt = np.zeros(out.shape, dtype=np.int32) if return_counts else None
-    fn = lib().oracle_siddon if projection_type in ("Siddon", "ray-voxel") else lib().oracle_interp
+    fn = lib().oracle_siddon if siddon else lib().oracle_interp
     fn(img.ctypes.data, C.byref(s), a0, a1, v0, v1, out.ctypes.data,
        cnt.ctypes.data if cnt is not None else None, _threads(nthreads))
     return (out, cnt) if return_counts else out
@@ -136,6 +146,10 @@ def atb(proj, geo, angles, backprojection_type="FDK", angle_range=None, z_range=
     proj = _f32(proj)
     assert proj.shape == (G.n, s.nDetecV, s.nDetecU)
     out = np.zeros((z1 - z0, s.nVoxelY, s.nVoxelX), dtype=np.float32)
+    if getattr(G.g, "mode", "cone") == "parallel":   # one parallel backprojector for both types
+        lib().oracle_backproject_parallel(proj.ctypes.data, C.byref(s), a0, a1, z0, z1, out.ctypes.data,
+                                          _threads(nthreads))
+        return out
     matched = 1 if backprojection_type == "matched" else 0
     lib().oracle_backproject(proj.ctypes.data, C.byref(s), a0, a1, z0, z1, matched, out.ctypes.data,
                              _threads(nthreads))

@@ -107,8 +107,8 @@ def _worker(spec_path):
         out = np.empty((n, geo.nDetecV, geo.nDetecU), dtype=np.float32)
         for _ in range(int(spec.get("repeat", 1))):
             t = time.perf_counter()
-            rc = L.ref_ax(inp.ctypes.data, C.byref(geo), out.ctypes.data, ang.ctypes.data, n,
-                          0 if op == "siddon" else 1, dev)
+            kind = (0 if op == "siddon" else 1) + (2 if spec.get("parallel") else 0)
+            rc = L.ref_ax(inp.ctypes.data, C.byref(geo), out.ctypes.data, ang.ctypes.data, n, kind, dev)
             times.append(time.perf_counter() - t)
             if rc:
                 raise SystemExit("reference returned %d" % rc)
@@ -120,8 +120,8 @@ def _worker(spec_path):
         out = np.empty((geo.nVoxelZ, geo.nVoxelY, geo.nVoxelX), dtype=np.float32)
         for _ in range(int(spec.get("repeat", 1))):
             t = time.perf_counter()
-            rc = L.ref_atb(inp.ctypes.data, C.byref(geo), out.ctypes.data, ang.ctypes.data, n,
-                           0 if op == "fdk" else 1, dev)
+            kind = 2 if spec.get("parallel") else (0 if op == "fdk" else 1)
+            rc = L.ref_atb(inp.ctypes.data, C.byref(geo), out.ctypes.data, ang.ctypes.data, n, kind, dev)
             times.append(time.perf_counter() - t)
             if rc:
                 raise SystemExit("reference returned %d" % rc)
@@ -163,12 +163,14 @@ def _run(op, inp, geo=None, angles=None, repeat=1, device=0, timeout=1800, **ext
 
 def ax(img, geo, angles, projection_type="Siddon", repeat=1, device=0):
     op = "interpolated" if projection_type == "interpolated" else "siddon"
-    return _run(op, img, geo, angles, repeat=repeat, device=device)
+    return _run(op, img, geo, angles, repeat=repeat, device=device,
+                parallel=getattr(geo, "mode", "cone") == "parallel")
 
 
 def atb(proj, geo, angles, backprojection_type="FDK", repeat=1, device=0):
     op = "matched" if backprojection_type == "matched" else "fdk"
-    return _run(op, proj, geo, angles, repeat=repeat, device=device)
+    return _run(op, proj, geo, angles, repeat=repeat, device=device,
+                parallel=getattr(geo, "mode", "cone") == "parallel")
 
 
 def pocs_tv(img, alpha, maxiter, repeat=1, device=0):

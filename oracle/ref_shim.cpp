@@ -15,10 +15,13 @@
 
 #if defined(REF_AX)
 #include "Siddon_projection.hpp"
+#include "Siddon_projection_parallel.hpp"
 #include "ray_interpolated_projection.hpp"
+#include "ray_interpolated_projection_parallel.hpp"
 #elif defined(REF_ATB)
 #include "voxel_backprojection.hpp"
 #include "voxel_backprojection2.hpp"
+#include "voxel_backprojection_parallel.hpp"
 #elif defined(REF_TV)
 #include "GD_TV.hpp"
 #endif
@@ -34,24 +37,33 @@ extern "C" {
 
 #if defined(REF_AX)
 // projector: 0 = Siddon (siddon_ray_projection, Siddon_projection.cu:271),
-//            1 = interpolated (interpolation_projection, ray_interpolated_projection.cu:211)
+//            1 = interpolated (interpolation_projection, ray_interpolated_projection.cu:211),
+//            2 = parallel Siddon (siddon_ray_projection_parallel),
+//            3 = parallel interpolated (interpolation_projection_parallel)
 int ref_ax(float* img, const Geometry* geo, float* out, const float* angles, int nangles, int projector, int dev) {
     OneGpu g(dev);
     const size_t npix = (size_t)geo->nDetecU * (size_t)geo->nDetecV;
     float** rows = (float**)std::malloc(sizeof(float*) * (size_t)nangles);
     if (!rows) return 1;
     for (int i = 0; i < nangles; ++i) rows[i] = out + npix * (size_t)i;
-    int rc = projector == 0 ? siddon_ray_projection(img, *geo, rows, angles, nangles, g.ids)
-                            : interpolation_projection(img, *geo, rows, angles, nangles, g.ids);
+    int rc = 1;
+    switch (projector) {
+        case 0: rc = siddon_ray_projection(img, *geo, rows, angles, nangles, g.ids); break;
+        case 1: rc = interpolation_projection(img, *geo, rows, angles, nangles, g.ids); break;
+        case 2: rc = siddon_ray_projection_parallel(img, *geo, rows, angles, nangles, g.ids); break;
+        case 3: rc = interpolation_projection_parallel(img, *geo, rows, angles, nangles, g.ids); break;
+    }
     std::free(rows);
     return rc;
 }
 #elif defined(REF_ATB)
 // backprojector: 0 = FDK (voxel_backprojection, voxel_backprojection.cu:293),
-//                1 = matched (voxel_backprojection2, voxel_backprojection2.cu:318)
+//                1 = matched (voxel_backprojection2, voxel_backprojection2.cu:318),
+//                2 = parallel (voxel_backprojection_parallel)
 int ref_atb(float* proj, const Geometry* geo, float* out, const float* angles, int nangles, int backprojector,
             int dev) {
     OneGpu g(dev);
+    if (backprojector == 2) return voxel_backprojection_parallel(proj, *geo, out, angles, nangles, g.ids);
     return backprojector == 0 ? voxel_backprojection(proj, *geo, out, angles, nangles, g.ids)
                               : voxel_backprojection2(proj, *geo, out, angles, nangles, g.ids);
 }

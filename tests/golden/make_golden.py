@@ -20,8 +20,11 @@ from tests import golden_cases as GC  # noqa: E402
 
 
 def main():
-    out_dir = os.path.dirname(os.path.abspath(__file__))
-    for name in GC.CASES:
+    # usage: make_golden.py [OUT_DIR [CASE ...]]   (default: this directory, every case)
+    out_dir = sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__))
+    names = sys.argv[2:] or GC.CASES
+    os.makedirs(out_dir, exist_ok=True)
+    for name in names:
         geo, ang, img = GC.make(name)
         res = {}
         res["siddon"], _ = ref.ax(img, geo, ang, "Siddon")

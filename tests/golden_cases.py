@@ -1,13 +1,13 @@
 """Small seeded cases whose reference outputs are stored in tests/golden/."""
 import numpy as np
 
-from tigre_b200.utilities.geometry import cone_geometry
+from tigre_b200.utilities.geometry import cone_geometry, geometry
 from tigre_b200.utilities.phantom import random_ellipsoids
 
 TV_ALPHA = 0.002
 TV_ITERS = 10
 
-CASES = ("small", "offsets")
+CASES = ("small", "offsets", "parallel")
 
 
 def make(name):
@@ -21,6 +21,17 @@ def make(name):
         geo.offDetector = np.array((1.2, -0.8))
         ang = np.linspace(0.1, 1.7 * np.pi, 10, endpoint=False).astype(np.float32)
         img = random_ellipsoids((24, 30, 28), seed=22)
+    elif name == "parallel":
+        # parallel beam with origin offsets, a horizontal detector offset and COR.  No vertical
+        # detector offset: the reference's parallel Siddon keeps one z index per ray
+        # (Siddon_projection_parallel.cu:224-266), so it is exact only for rays without a
+        # z component, which a vertical offset would give (its source is not offset).
+        geo = geometry(mode="parallel", nVoxel=np.array([20, 26, 30]))
+        geo.offOrigin = np.array((0.5, -1.0, 1.5))
+        geo.offDetector = np.array((0.0, 0.6))
+        geo.COR = 0.3
+        ang = np.linspace(0.05, np.pi, 9, endpoint=False).astype(np.float32)
+        img = random_ellipsoids((20, 26, 30), seed=23)
     else:
         raise KeyError(name)
     return geo, ang, img.astype(np.float32)

@@ -19,6 +19,7 @@ LIB_PATH = os.path.join(_PKG, "libtigre_b200.so")
 F32, BF16, F16 = 0, 1, 2
 PROJ_SIDDON, PROJ_INTERPOLATED = 0, 1
 BACKPROJ_FDK, BACKPROJ_MATCHED = 0, 1
+PLAN_PARALLEL = 1
 
 _FP = C.POINTER(C.c_float)
 
@@ -72,6 +73,7 @@ _SIGS = {
     "tigre_interpolation_projection_parallel": (C.c_int, [C.c_void_p] * 4 + [C.c_int, C.c_void_p, C.c_int]),
     "tigre_voxel_backprojection_parallel": (C.c_int, [C.c_void_p] * 4 + [C.c_int, C.c_void_p, C.c_int]),
     "tigre_plan_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "tigre_plan_create_ex": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "tigre_plan_destroy": (None, [C.c_void_p]),
     "tigre_plan_scratch_bytes": (C.c_longlong, [C.c_void_p]),
     "tigre_plan_status": (C.c_int, [C.c_void_p, C.c_int]),
@@ -181,6 +183,7 @@ def _geo_key(g, device):
         h.update(str(a.dtype).encode() + str(a.shape).encode())
         h.update(a.tobytes())
     h.update(str(float(g.accuracy)).encode())
+    h.update(str(getattr(g, "mode", "cone")).encode())
     h.update(str(device).encode())
     return h.hexdigest()
 
@@ -195,8 +198,9 @@ class Plan:
         self.device = int(device)
         self._cg = CGeometry(geo_checked, self.n)
         h = C.c_void_p()
-        check(lib().tigre_plan_create(C.byref(self._cg.s), self.angles.ctypes.data, self.n, self.device,
-                                      C.byref(h)), "tigre_plan_create")
+        self.parallel = getattr(geo_checked, "mode", "cone") == "parallel"
+        check(lib().tigre_plan_create_ex(C.byref(self._cg.s), self.angles.ctypes.data, self.n, self.device,
+                                         PLAN_PARALLEL if self.parallel else 0, C.byref(h)), "tigre_plan_create_ex")
         self.handle = h
         self.vol_shape = tuple(int(v) for v in geo_checked.nVoxel)
         self.det_shape = tuple(int(v) for v in geo_checked.nDetector)

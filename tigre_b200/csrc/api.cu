@@ -120,6 +120,9 @@ int tigre_atb_ex(TigrePlan* plan, const void* d_proj, int pdt, void* d_vol, int 
     if (!dtype_ok(vdt) || !dtype_ok(pdt)) return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype");
     if (backprojector != TIGRE_BACKPROJ_FDK && backprojector != TIGRE_BACKPROJ_MATCHED)
         return fail(TIGRE_ERR_BAD_ASSERT, "unknown backprojector");
+    // parallel beam has one backprojector (voxel_backprojection_parallel); its frames are
+    // encoded for the FDK path (unit weight, no scale)
+    if (plan->parallel) backprojector = TIGRE_BACKPROJ_FDK;
     DeviceGuard g(plan->device);
     cudaStream_t st = (cudaStream_t)stream;
     const Dims& d = plan->d;
@@ -227,12 +230,12 @@ struct DeviceState {
         *out = buf[slot];
         return TIGRE_SUCCESS;
     }
-    int plan(const TigreGeometry* g, const float* angles, int n, int dev, TigrePlan** out) {
-        const uint64_t k = geometry_key(g, angles, n);
+    int plan(const TigreGeometry* g, const float* angles, int n, int dev, int flags, TigrePlan** out) {
+        const uint64_t k = fnv(geometry_key(g, angles, n), &flags, sizeof(flags));
         for (auto& e : plans)
             if (e.key == k) { *out = e.plan; return TIGRE_SUCCESS; }
         TigrePlan* p = nullptr;
-        if (int rc = tigre_plan_create(g, angles, n, dev, &p)) return rc;
+        if (int rc = tigre_plan_create_ex(g, angles, n, dev, flags, &p)) return rc;
         if (plans.size() >= 4) {
             cudaStreamSynchronize(st);
             tigre_plan_destroy(plans.front().plan);
@@ -272,7 +275,7 @@ size_t chunk_views(size_t per_view_bytes, int nangles) {
 }
 
 int host_project(const float* img, const TigreGeometry* geo, float* const* result, const float* angles, int nangles,
-                 const int* ids, int n, int projector) {
+                 const int* ids, int n, int projector, int flags = 0) {
     if (!img || !geo || !result || !angles) return fail(TIGRE_ERR_BAD_ASSERT, "null argument");
     int dev = 0;
     if (int rc = pick_device(ids, n, &dev)) return rc;
@@ -281,7 +284,7 @@ int host_project(const float* img, const TigreGeometry* geo, float* const* resul
     std::lock_guard<std::mutex> lk(S->mu);
     if (int rc = S->init(dev)) return rc;
     TigrePlan* plan = nullptr;
-    if (int rc = S->plan(geo, angles, nangles, dev, &plan)) return rc;
+    if (int rc = S->plan(geo, angles, nangles, dev, flags, &plan)) return rc;
     const Dims& d = plan->d;
     const size_t nvox = (size_t)d.nX * d.nY * d.nZ, npix = (size_t)d.nU * d.nV;
     void* dvol = nullptr;
@@ -311,7 +314,7 @@ int host_project(const float* img, const TigreGeometry* geo, float* const* resul
 }
 
 int host_backproject(const float* proj, const TigreGeometry* geo, float* result, const float* angles, int nangles,
-                     const int* ids, int n, int matched) {
+                     const int* ids, int n, int matched, int flags = 0) {
     if (!proj || !geo || !result || !angles) return fail(TIGRE_ERR_BAD_ASSERT, "null argument");
     int dev = 0;
     if (int rc = pick_device(ids, n, &dev)) return rc;
@@ -320,7 +323,7 @@ int host_backproject(const float* proj, const TigreGeometry* geo, float* result,
     std::lock_guard<std::mutex> lk(S->mu);
     if (int rc = S->init(dev)) return rc;
     TigrePlan* plan = nullptr;
-    if (int rc = S->plan(geo, angles, nangles, dev, &plan)) return rc;
+    if (int rc = S->plan(geo, angles, nangles, dev, flags, &plan)) return rc;
     const Dims& d = plan->d;
     const size_t nvox = (size_t)d.nX * d.nY * d.nZ, npix = (size_t)d.nU * d.nV;
     void* dvol = nullptr;
@@ -412,19 +415,19 @@ int tigre_pocs_tv(const float* img, float* dst, float alpha, const long* image_s
     return host_pocs_tv(img, dst, alpha, image_size, max_iter, ids, n);
 }
 
-int tigre_siddon_ray_projection_parallel(const float*, const TigreGeometry*, float* const*, const float*, int,
-                                         const int*, int) {
-    return fail(TIGRE_ERR_BAD_ASSERT, "parallel-beam projection is not provided by libtigre_b200");
+int tigre_siddon_ray_projection_parallel(const float* img, const TigreGeometry* geo, float* const* result,
+                                         const float* angles, int nangles, const int* ids, int n) {
+    return host_project(img, geo, result, angles, nangles, ids, n, TIGRE_PROJ_SIDDON, TIGRE_PLAN_PARALLEL);
 }
 
-int tigre_interpolation_projection_parallel(const float*, const TigreGeometry*, float* const*, const float*, int,
-                                            const int*, int) {
-    return fail(TIGRE_ERR_BAD_ASSERT, "parallel-beam projection is not provided by libtigre_b200");
+int tigre_interpolation_projection_parallel(const float* img, const TigreGeometry* geo, float* const* result,
+                                            const float* angles, int nangles, const int* ids, int n) {
+    return host_project(img, geo, result, angles, nangles, ids, n, TIGRE_PROJ_INTERPOLATED, TIGRE_PLAN_PARALLEL);
 }
 
-int tigre_voxel_backprojection_parallel(const float*, const TigreGeometry*, float*, const float*, int, const int*,
-                                        int) {
-    return fail(TIGRE_ERR_BAD_ASSERT, "parallel-beam backprojection is not provided by libtigre_b200");
+int tigre_voxel_backprojection_parallel(const float* proj, const TigreGeometry* geo, float* result,
+                                        const float* angles, int nangles, const int* ids, int n) {
+    return host_backproject(proj, geo, result, angles, nangles, ids, n, 0, TIGRE_PLAN_PARALLEL);
 }
 
 }  // extern "C"

@@ -36,6 +36,7 @@ struct InterpArgs {
     int a0;
     int nX, nY, nZ, nU, nV;
     double dVX, dVY, dVZ, acc;
+    int parallel;        // parallel beam: each pixel's source is s + u du + v dv
 };
 
 // one corner quad (fast axis x z 2x2 block) as floats
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs p) {
     double d[3], s[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        s[k] = F.s[k];
+        s[k] = p.parallel ? fma(pv, F.dv[k], fma((double)u, F.du[k], F.s[k])) : F.s[k];
         d[k] = fma(pv, F.dv[k], fma((double)u, F.du[k], F.o[k])) - s[k];
     }
     const double len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
@@ -209,6 +210,7 @@ int launch_interp(TigrePlan* P, const void* vol_x, const void* vol_y, const void
     a.vol_x = vol_x; a.vol_y = vol_y; a.quad_x = quad_x; a.quad_y = quad_y; a.frames = P->d_interp;
     a.nX = P->d.nX; a.nY = P->d.nY; a.nZ = P->d.nZ; a.nU = P->d.nU; a.nV = P->d.nV;
     a.dVX = P->d.dVX; a.dVY = P->d.dVY; a.dVZ = P->d.dVZ; a.acc = P->d.accuracy;
+    a.parallel = P->parallel ? 1 : 0;
     const bool nearest = P->d.accuracy > 1.0;
     const int rows = 8;
     dim3 block(32, rows);

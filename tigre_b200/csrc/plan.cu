@@ -107,25 +107,29 @@ void cells_bounds(TigrePlan* plan) {
     double slope = 0.0, span = 0.0;
     for (const FrameSiddon& f : plan->h_siddon) {
         for (int u = 0; u < d.nU; ++u) {
-            double rx = std::fma((double)u, f.du[0], f.o[0]) - f.s[0];
-            double ry = std::fma((double)u, f.du[1], f.o[1]) - f.s[1];
+            // the kernels' ray setup; in parallel beam each pixel has its own source
+            const double sx = plan->parallel ? std::fma((double)u, f.du[0], f.s[0]) : f.s[0];
+            const double sy = plan->parallel ? std::fma((double)u, f.du[1], f.s[1]) : f.s[1];
+            double rx = std::fma((double)u, f.du[0], f.o[0]) - sx;
+            double ry = std::fma((double)u, f.du[1], f.o[1]) - sy;
             if (std::fabs(rx) < 0.001) rx = 0.0;
             if (std::fabs(ry) < 0.001) ry = 0.0;
             double am = -1e300, aM = 1e300;
             bool miss = false;
             if (rx != 0.0) {
-                const double i = 1.0 / rx, a0 = -f.s[0] * i, a1 = ((double)d.nX - f.s[0]) * i;
+                const double i = 1.0 / rx, a0 = -sx * i, a1 = ((double)d.nX - sx) * i;
                 am = std::fmax(am, std::fmin(a0, a1)); aM = std::fmin(aM, std::fmax(a0, a1));
-            } else if (f.s[0] < 0.0 || f.s[0] > (double)d.nX) miss = true;
+            } else if (sx < 0.0 || sx > (double)d.nX) miss = true;
             if (ry != 0.0) {
-                const double i = 1.0 / ry, a0 = -f.s[1] * i, a1 = ((double)d.nY - f.s[1]) * i;
+                const double i = 1.0 / ry, a0 = -sy * i, a1 = ((double)d.nY - sy) * i;
                 am = std::fmax(am, std::fmin(a0, a1)); aM = std::fmin(aM, std::fmax(a0, a1));
-            } else if (f.s[1] < 0.0 || f.s[1] > (double)d.nY) miss = true;
+            } else if (sy < 0.0 || sy > (double)d.nY) miss = true;
             if (miss || !(am < aM)) continue;
             const double dom = std::max(std::fabs(rx), std::fabs(ry));
             for (int e = 0; e < 2; ++e) {
                 const double pv = e ? 0.0 : (double)(d.nV - 1);
-                double rz = std::fma(pv, f.dv[2], std::fma((double)u, f.du[2], f.o[2])) - f.s[2];
+                const double sz = plan->parallel ? std::fma(pv, f.dv[2], std::fma((double)u, f.du[2], f.s[2])) : f.s[2];
+                double rz = std::fma(pv, f.dv[2], std::fma((double)u, f.du[2], f.o[2])) - sz;
                 if (std::fabs(rz) < 0.001) rz = 0.0;
                 slope = std::max(slope, dom > 0.0 ? std::fabs(rz) / dom : 1e30);
                 span = std::max(span, (aM - am) * std::fabs(rz));
@@ -134,11 +138,107 @@ void cells_bounds(TigrePlan* plan) {
     }
     plan->cells_slope_max = slope;
     plan->cells_zspan_max = span;
+    // the exact slope also governs the one-crossing variant of the stepped column kernel
+    plan->column_slope_max = std::max(plan->column_slope_max, slope);
     // one z crossing per xy cell at most (z change per cell < 1, with margin), and pads that
     // stay a modest multiple of the volume
     const double pad = std::ceil(span) + 3.0;
     const bool ok = slope < 0.9 && pad <= 2.0 * d.nZ + 256.0 && std::getenv("TIGRE_B200_NO_CELLS") == nullptr;
     plan->cells_zpad = ok ? (int)pad : 0;
+}
+
+// Parallel-beam frames.  Every pixel has its own source: source(u, v) = s + u du + v dv.
+//  * Siddon (computeDeltas_Siddon_parallel, Siddon_projection_parallel.cu:388-480): pixel
+//    (0,0) on the plane x = DSO; rotation about z by alpha only; the detector offset moves
+//    the detector points, not the source.
+//  * interpolated (computeDeltas_parallel, ray_interpolated_projection_parallel.cu:309-400):
+//    full ZYZ Euler rotation, detector offset applied twice (:341-356), voxel centres at
+//    integers; sample cap with dVoxelX (:175-176).
+//  * backprojection (computeDeltasCubeParallel, voxel_backprojection_parallel.cu:510-585, the
+//    steps of the cone frame): the voxel projects orthographically, u = y - COR/dDetecU + nU/2
+//    and v = z + nV/2 in texture coordinates, weight 1 (:221-250).  This is encoded in the cone
+//    FDK frame: the depth row is made constant 1 (o.x = dx.x = dy.x = dz.x = 0, s.x = -1), the
+//    numerator DSO - DSD - s.x is 1 (DSO = DSD = 1), s.y = s.z = 0 and the FDK weight's
+//    sin/cos are 0, so t = 1 and the weight is 1 exactly.
+void parallel_frames(const TigreGeometry* g, const Dims& d, int i, double al, double th, double ps, TigrePlan* plan) {
+    const double dso = g->DSO[i], dsd = g->DSD[i];
+    const double offx = at(g->offOrigX, i), offy = at(g->offOrigY, i), offz = at(g->offOrigZ, i);
+    const double offu = at(g->offDetecU, i), offv = at(g->offDetecV, i);
+    const double cor = at(g->COR, i);
+    const Rot3 rd = detector_rotation(at(g->dRoll, i), at(g->dPitch, i), at(g->dYaw, i));
+    const double y0 = d.dDU * (-(double)d.nU / 2.0 + 0.5), z0 = d.dDV * ((double)d.nV / 2.0 - 0.5);
+    const double corx = -cor * std::sin(al) / d.dVX, cory = cor * std::cos(al) / d.dVY;
+    auto frame = [&](const Rot3& rot, double offmul, double centre, double o3[3], double du3[3], double dv3[3],
+                     double s3[3]) {
+        Vec P{0.0, y0, z0}, Pu{0.0, y0 + d.dDU, z0}, Pv{0.0, y0, z0 - d.dDV}, S{0.0, y0, z0};
+        for (Vec* q : {&P, &Pu, &Pv}) {
+            *q = rd.apply(*q);
+            q->x -= (dsd - dso);
+            q->y += offmul * offu;
+            q->z += offmul * offv;
+        }
+        S = rd.apply(S);
+        S.x += dso;
+        for (Vec* q : {&P, &Pu, &Pv, &S}) {
+            *q = rot.apply(*q);
+            q->x = (q->x - offx + d.sVX / 2 - centre * d.dVX) / d.dVX + corx;
+            q->y = (q->y - offy + d.sVY / 2 - centre * d.dVY) / d.dVY + cory;
+            q->z = (q->z - offz + d.sVZ / 2 - centre * d.dVZ) / d.dVZ;
+        }
+        o3[0] = P.x; o3[1] = P.y; o3[2] = P.z;
+        du3[0] = Pu.x - P.x; du3[1] = Pu.y - P.y; du3[2] = Pu.z - P.z;
+        dv3[0] = Pv.x - P.x; dv3[1] = Pv.y - P.y; dv3[2] = Pv.z - P.z;
+        s3[0] = S.x; s3[1] = S.y; s3[2] = S.z;
+    };
+    FrameSiddon& fs = plan->h_siddon[i];
+    frame(euler_zyz(al, 0.0, 0.0), 1.0, 0.0, fs.o, fs.du, fs.dv, fs.s);
+    fs.layout = std::fabs(fs.du[1]) >= std::fabs(fs.du[0]) ? 1 : 0;
+    fs.pad_ = 0;
+    FrameInterp& fi = plan->h_interp[i];
+    frame(euler_zyz(al, th, ps), 2.0, 0.5, fi.o, fi.du, fi.dv, fi.s);
+    fi.layout = std::fabs(fi.du[1]) >= std::fabs(fi.du[0]) ? 1 : 0;
+    fi.pad_ = 0;
+    {
+        // maxdistanceCuboid as for cone beam; cap with dVoxelX
+        const double mx = (double)(d.nX / 2) + std::fabs(offx) / d.dVX;
+        const double my = (double)(d.nY / 2) + std::fabs(offy) / d.dVY;
+        const double mz = (double)(d.nZ / 2) + std::fabs(offz) / d.dVZ;
+        const double a = dso / d.dVX, b = dso / d.dVY;
+        double md;
+        if (th == 0.0 && ps == 0.0) {
+            const double sa = std::sin(al), ca = std::cos(al);
+            md = a * b / std::sqrt(a * a * sa * sa + b * b * ca * ca) - std::sqrt(mx * mx + my * my);
+        } else {
+            md = dso / std::max(std::max(d.dVX, d.dVY), d.dVZ) - std::sqrt(mx * mx + my * my + mz * mz);
+        }
+        const double crop = std::floor(std::max(md, 0.0));
+        fi.first_sample = std::floor(crop / d.accuracy);
+        fi.cap = (2.0 * dso / d.dVX + crop) / d.accuracy;
+    }
+    // backprojection frame: the cone frame's steps, then the orthographic encoding
+    const Rot3 rt = euler_zyz_T(-al, -th, -ps);
+    const Rot3 rdt = rd.transposed();
+    Vec Q{-(d.sVX / 2 - d.dVX / 2) + offx, -(d.sVY / 2 - d.dVY / 2) + offy, -(d.sVZ / 2 - d.dVZ / 2) + offz};
+    Vec pts[4] = {Q, {Q.x + d.dVX, Q.y, Q.z}, {Q.x, Q.y + d.dVY, Q.z}, {Q.x, Q.y, Q.z + d.dVZ}};
+    const double off = dsd - dso;
+    for (Vec& q : pts) {
+        q = rt.apply(q);
+        q.z -= offv; q.y -= offu;
+        q.x += off;
+        q = rdt.apply(q);
+        q.x -= off;
+        q.z /= d.dDV; q.y /= d.dDU;
+    }
+    FrameBP& fb = plan->h_bp[i];
+    fb.o[0] = 0.0; fb.o[1] = pts[0].y; fb.o[2] = pts[0].z;
+    fb.dx[0] = 0.0; fb.dx[1] = pts[1].y - pts[0].y; fb.dx[2] = pts[1].z - pts[0].z;
+    fb.dy[0] = 0.0; fb.dy[1] = pts[2].y - pts[0].y; fb.dy[2] = pts[2].z - pts[0].z;
+    fb.dz[0] = 0.0; fb.dz[1] = pts[3].y - pts[0].y; fb.dz[2] = pts[3].z - pts[0].z;
+    fb.s[0] = -1.0; fb.s[1] = 0.0; fb.s[2] = 0.0;
+    fb.sina = 0.f; fb.cosa = 0.f;
+    fb.cor = (float)cor; fb.dsd = 1.f; fb.dso = 1.f;
+    fb.offx = (float)offx; fb.offy = (float)offy; fb.offz = (float)offz;
+    fb.offu = (float)offu; fb.offv = (float)offv;
 }
 
 int compute_frames(const TigreGeometry* g, const float* angles, int nangles, TigrePlan* plan) {
@@ -172,6 +272,13 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
         const Rot3 rd = detector_rotation(at(g->dRoll, i), at(g->dPitch, i), at(g->dYaw, i));
         const Rot3 re = euler_zyz(al, th, ps);
 
+        if (plan->parallel) {
+            parallel_frames(g, d, i, al, th, ps, plan);
+            if (plan->h_siddon[i].dv[0] != 0.0 || plan->h_siddon[i].dv[1] != 0.0) columns = false;
+            const FrameBP& fb = plan->h_bp[i];
+            if (std::fabs(fb.dz[0]) > 1e-12 * d.dVZ || std::fabs(fb.dz[1]) > 1e-12 * d.dVZ) axial = false;
+            continue;
+        }
         // ---- Siddon frame (computeDeltas_Siddon) ----
         Vec S{dso, 0.0, 0.0};
         Vec P{0.0, d.dDU * (-(double)d.nU / 2.0 + 0.5), d.dDV * ((double)d.nV / 2.0 - 0.5)};
@@ -392,14 +499,21 @@ int tigre_version(void) { return 100; }
 unsigned long long tigre_launch_count(void) { return tigre::g_launches.load(std::memory_order_relaxed); }
 
 int tigre_plan_create(const TigreGeometry* geo, const float* angles, int nangles, int device, TigrePlan** out) {
+    return tigre_plan_create_ex(geo, angles, nangles, device, 0, out);
+}
+
+int tigre_plan_create_ex(const TigreGeometry* geo, const float* angles, int nangles, int device, int flags,
+                         TigrePlan** out) {
     if (!out) return fail(TIGRE_ERR_BAD_ASSERT, "null output plan pointer");
     *out = nullptr;
+    if (flags & ~TIGRE_PLAN_PARALLEL) return fail(TIGRE_ERR_BAD_ASSERT, "unknown plan flags");
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0) return fail(TIGRE_ERR_NO_CAPABLE_DEVICES, "no CUDA device available");
     if (device < 0 || device >= ndev) return fail(TIGRE_ERR_BAD_ASSERT, "device id out of range");
     TigrePlan* p = new TigrePlan();
     p->device = device;
+    p->parallel = (flags & TIGRE_PLAN_PARALLEL) != 0;
     int rc = compute_frames(geo, angles, nangles, p);
     if (rc) { delete p; return rc; }
     int prev = 0;

@@ -38,6 +38,7 @@ struct SiddonArgs {
     double dVX, dVY, dVZ;
     unsigned long long* count;   // segment-count mode
     int zpad;                    // zero slices before and after each z-run of the z-fast copy
+    int parallel;                // parallel beam: each pixel's source is s + u du + v dv
     int* status;                 // plan status word (bit 1: a ray outside the host's z bound)
 };
 
@@ -88,6 +89,7 @@ __device__ __forceinline__ AxisSetup axis_setup(double s, double r, double am, d
 struct RaySetup {
     bool hit;
     double r[3];
+    double s[3];   // source of this ray (the view's source, or the pixel's in parallel beam)
     double am, aM;
 };
 
@@ -96,7 +98,8 @@ __device__ __forceinline__ RaySetup ray_setup(const SiddonArgs& p, const FrameSi
     const double pv = (double)(p.nV - 1 - v);   // detector v flip, Siddon_projection.cu:141
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        R.r[k] = fma(pv, F.dv[k], fma((double)u, F.du[k], F.o[k])) - F.s[k];
+        R.s[k] = p.parallel ? fma(pv, F.dv[k], fma((double)u, F.du[k], F.s[k])) : F.s[k];
+        R.r[k] = fma(pv, F.dv[k], fma((double)u, F.du[k], F.o[k])) - R.s[k];
         if (fabs(R.r[k]) < 0.001) R.r[k] = 0.0;   // Siddon_projection.cu:156-159
     }
     const int n[3] = {p.nX, p.nY, p.nZ};
@@ -106,10 +109,10 @@ __device__ __forceinline__ RaySetup ray_setup(const SiddonArgs& p, const FrameSi
     for (int k = 0; k < 3; ++k) {
         if (R.r[k] != 0.0) {
             const double inv = 1.0 / R.r[k];
-            const double a0 = -F.s[k] * inv, a1 = ((double)n[k] - F.s[k]) * inv;
+            const double a0 = -R.s[k] * inv, a1 = ((double)n[k] - R.s[k]) * inv;
             am = fmax(am, fmin(a0, a1));
             aM = fmin(aM, fmax(a0, a1));
-        } else if (F.s[k] < 0.0 || F.s[k] > (double)n[k]) {
+        } else if (R.s[k] < 0.0 || R.s[k] > (double)n[k]) {
             miss = true;
         }
     }
@@ -132,9 +135,9 @@ __global__ void __launch_bounds__(256) siddon_kernel(SiddonArgs p) {
         ((TP*)p.proj)[oidx] = from_f32<TP>(0.f);
         return;
     }
-    const AxisSetup ax = axis_setup(F.s[0], R.r[0], R.am, R.aM, p.nX);
-    const AxisSetup ay = axis_setup(F.s[1], R.r[1], R.am, R.aM, p.nY);
-    const AxisSetup az = axis_setup(F.s[2], R.r[2], R.am, R.aM, p.nZ);
+    const AxisSetup ax = axis_setup(R.s[0], R.r[0], R.am, R.aM, p.nX);
+    const AxisSetup ay = axis_setup(R.s[1], R.r[1], R.am, R.aM, p.nY);
+    const AxisSetup az = axis_setup(R.s[2], R.r[2], R.am, R.aM, p.nZ);
     // strides of the working layout chosen for this view
     const int layout = F.layout;
     const TV* vol = (const TV*)(layout ? p.vol_y : p.vol_x);
@@ -187,9 +190,9 @@ __global__ void __launch_bounds__(256) siddon_count_kernel(SiddonArgs p) {
         const FrameSiddon& F = p.frames[p.a0 + blockIdx.z];
         const RaySetup R = ray_setup(p, F, u, v);
         if (R.hit) {
-            const AxisSetup ax = axis_setup(F.s[0], R.r[0], R.am, R.aM, p.nX);
-            const AxisSetup ay = axis_setup(F.s[1], R.r[1], R.am, R.aM, p.nY);
-            const AxisSetup az = axis_setup(F.s[2], R.r[2], R.am, R.aM, p.nZ);
+            const AxisSetup ax = axis_setup(R.s[0], R.r[0], R.am, R.aM, p.nX);
+            const AxisSetup ay = axis_setup(R.s[1], R.r[1], R.am, R.aM, p.nY);
+            const AxisSetup az = axis_setup(R.s[2], R.r[2], R.am, R.aM, p.nZ);
             c = 1 + ax.ncross + ay.ncross + az.ncross;
         }
     }
@@ -221,21 +224,24 @@ __global__ void __launch_bounds__(128, 6) siddon_columns_kernel(SiddonArgs p) {
     const FrameSiddon& F = p.frames[p.a0 + la];
     const int vbase = blockIdx.z * (32 * R) + lane;
     TP* out = (TP*)p.proj + (size_t)la * p.nV * p.nU + u;
-    // ---- shared xy ray (identical in every lane of the warp) ----
-    double rx = fma((double)u, F.du[0], F.o[0]) - F.s[0];
-    double ry = fma((double)u, F.du[1], F.o[1]) - F.s[1];
+    // ---- shared xy ray (identical in every lane of the warp); in parallel beam the column's
+    // source is s + u du (dv has no xy part on this path) ----
+    const double sx = p.parallel ? fma((double)u, F.du[0], F.s[0]) : F.s[0];
+    const double sy = p.parallel ? fma((double)u, F.du[1], F.s[1]) : F.s[1];
+    double rx = fma((double)u, F.du[0], F.o[0]) - sx;
+    double ry = fma((double)u, F.du[1], F.o[1]) - sy;
     if (fabs(rx) < 0.001) rx = 0.0;   // Siddon_projection.cu:156-159
     if (fabs(ry) < 0.001) ry = 0.0;
     double am = -1e300, aM = 1e300;
     bool miss = false;
     if (rx != 0.0) {
-        const double i = 1.0 / rx, a0 = -F.s[0] * i, a1 = ((double)p.nX - F.s[0]) * i;
+        const double i = 1.0 / rx, a0 = -sx * i, a1 = ((double)p.nX - sx) * i;
         am = fmax(am, fmin(a0, a1)); aM = fmin(aM, fmax(a0, a1));
-    } else if (F.s[0] < 0.0 || F.s[0] > (double)p.nX) miss = true;
+    } else if (sx < 0.0 || sx > (double)p.nX) miss = true;
     if (ry != 0.0) {
-        const double i = 1.0 / ry, a0 = -F.s[1] * i, a1 = ((double)p.nY - F.s[1]) * i;
+        const double i = 1.0 / ry, a0 = -sy * i, a1 = ((double)p.nY - sy) * i;
         am = fmax(am, fmin(a0, a1)); aM = fmin(aM, fmax(a0, a1));
-    } else if (F.s[1] < 0.0 || F.s[1] > (double)p.nY) miss = true;
+    } else if (sy < 0.0 || sy > (double)p.nY) miss = true;
     if (miss || !(am < aM)) {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -244,8 +250,8 @@ __global__ void __launch_bounds__(128, 6) siddon_columns_kernel(SiddonArgs p) {
         }
         return;
     }
-    const AxisSetup ax = axis_setup(F.s[0], rx, am, aM, p.nX);
-    const AxisSetup ay = axis_setup(F.s[1], ry, am, aM, p.nY);
+    const AxisSetup ax = axis_setup(sx, rx, am, aM, p.nX);
+    const AxisSetup ay = axis_setup(sy, ry, am, aM, p.nY);
     const int ncells = 1 + (int)ax.ncross + (int)ay.ncross;
     const float T = (float)(aM - am);
     // ---- per-row z state ----
@@ -255,9 +261,10 @@ __global__ void __launch_bounds__(128, 6) siddon_columns_kernel(SiddonArgs p) {
     for (int r = 0; r < R; ++r) {
         const int v = min(vbase + 32 * r, p.nV - 1);
         const double pv = (double)(p.nV - 1 - v);
-        double rz = fma(pv, F.dv[2], fma((double)u, F.du[2], F.o[2])) - F.s[2];
+        const double srcz = p.parallel ? fma(pv, F.dv[2], fma((double)u, F.du[2], F.s[2])) : F.s[2];
+        double rz = fma(pv, F.dv[2], fma((double)u, F.du[2], F.o[2])) - srcz;
         if (fabs(rz) < 0.001) rz = 0.0;
-        const double ze = fma(am, rz, F.s[2]);
+        const double ze = fma(am, rz, srcz);
         int z = (int)fmin(fmax(floor(ze), -1.0), (double)p.nZ);
         iz[r] = z;
         sum[r] = 0.f;
@@ -265,11 +272,11 @@ __global__ void __launch_bounds__(128, 6) siddon_columns_kernel(SiddonArgs p) {
         len[r] = (float)sqrt(rx * rx * p.dVX * p.dVX + ry * ry * p.dVY * p.dVY + rz * rz * p.dVZ * p.dVZ);
         if (rz > 0.0 && z < p.nZ) {
             sz[r] = 1;
-            tz0[r] = (float)(((double)(z + 1) - F.s[2]) / rz - am);
+            tz0[r] = (float)(((double)(z + 1) - srcz) / rz - am);
             dtz[r] = (float)(1.0 / rz);
         } else if (rz < 0.0 && z >= 0) {
             sz[r] = -1;
-            tz0[r] = (float)(((double)z - F.s[2]) / rz - am);
+            tz0[r] = (float)(((double)z - srcz) / rz - am);
             dtz[r] = (float)(-1.0 / rz);
         } else {
             sz[r] = 0;
@@ -392,20 +399,22 @@ __global__ void __launch_bounds__(128, 6) siddon_cells_kernel(SiddonArgs p) {
     const int vbase = blockIdx.z * (32 * R) + lane;
     TP* out = (TP*)p.proj + (size_t)la * p.nV * p.nU + u;
     // ---- shared xy ray ----
-    double rx = fma((double)u, F.du[0], F.o[0]) - F.s[0];
-    double ry = fma((double)u, F.du[1], F.o[1]) - F.s[1];
+    const double sx = p.parallel ? fma((double)u, F.du[0], F.s[0]) : F.s[0];
+    const double sy = p.parallel ? fma((double)u, F.du[1], F.s[1]) : F.s[1];
+    double rx = fma((double)u, F.du[0], F.o[0]) - sx;
+    double ry = fma((double)u, F.du[1], F.o[1]) - sy;
     if (fabs(rx) < 0.001) rx = 0.0;   // Siddon_projection.cu:156-159
     if (fabs(ry) < 0.001) ry = 0.0;
     double am = -1e300, aM = 1e300;
     bool miss = false;
     if (rx != 0.0) {
-        const double i = 1.0 / rx, a0 = -F.s[0] * i, a1 = ((double)p.nX - F.s[0]) * i;
+        const double i = 1.0 / rx, a0 = -sx * i, a1 = ((double)p.nX - sx) * i;
         am = fmax(am, fmin(a0, a1)); aM = fmin(aM, fmax(a0, a1));
-    } else if (F.s[0] < 0.0 || F.s[0] > (double)p.nX) miss = true;
+    } else if (sx < 0.0 || sx > (double)p.nX) miss = true;
     if (ry != 0.0) {
-        const double i = 1.0 / ry, a0 = -F.s[1] * i, a1 = ((double)p.nY - F.s[1]) * i;
+        const double i = 1.0 / ry, a0 = -sy * i, a1 = ((double)p.nY - sy) * i;
         am = fmax(am, fmin(a0, a1)); aM = fmin(aM, fmax(a0, a1));
-    } else if (F.s[1] < 0.0 || F.s[1] > (double)p.nY) miss = true;
+    } else if (sy < 0.0 || sy > (double)p.nY) miss = true;
     if (miss || !(am < aM)) {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -414,8 +423,8 @@ __global__ void __launch_bounds__(128, 6) siddon_cells_kernel(SiddonArgs p) {
         }
         return;
     }
-    const AxisSetup ax = axis_setup(F.s[0], rx, am, aM, p.nX);
-    const AxisSetup ay = axis_setup(F.s[1], ry, am, aM, p.nY);
+    const AxisSetup ax = axis_setup(sx, rx, am, aM, p.nX);
+    const AxisSetup ay = axis_setup(sy, ry, am, aM, p.nY);
     const int ncells = 1 + (int)ax.ncross + (int)ay.ncross;
     const double Td = aM - am;
     const float T = (float)Td;
@@ -426,9 +435,10 @@ __global__ void __launch_bounds__(128, 6) siddon_cells_kernel(SiddonArgs p) {
     for (int r = 0; r < R; ++r) {
         const int v = min(vbase + 32 * r, p.nV - 1);
         const double pv = (double)(p.nV - 1 - v);
-        double rzd = fma(pv, F.dv[2], fma((double)u, F.du[2], F.o[2])) - F.s[2];
+        const double szr = p.parallel ? fma(pv, F.dv[2], fma((double)u, F.du[2], F.s[2])) : F.s[2];
+        double rzd = fma(pv, F.dv[2], fma((double)u, F.du[2], F.o[2])) - szr;
         if (fabs(rzd) < 0.001) rzd = 0.0;
-        const double za = fma(am, rzd, F.s[2]) + P;   // z + pad at the xy entry
+        const double za = fma(am, rzd, szr) + P;   // z + pad at the xy entry
         const double zb = fma(Td, rzd, za);           // ... and at the xy exit
         const double lo = fmin(za, zb), hi = fmax(za, zb);
         bool live = hi > P && lo < P + (double)p.nZ;
@@ -527,7 +537,8 @@ __global__ void __launch_bounds__(128, 6) siddon_cells_kernel(SiddonArgs p) {
         const int v = vbase + 32 * r;
         if (v < p.nV) {
             const double pv = (double)(p.nV - 1 - v);
-            double rzd = fma(pv, F.dv[2], fma((double)u, F.du[2], F.o[2])) - F.s[2];
+            const double szr = p.parallel ? fma(pv, F.dv[2], fma((double)u, F.du[2], F.s[2])) : F.s[2];
+            double rzd = fma(pv, F.dv[2], fma((double)u, F.du[2], F.o[2])) - szr;
             if (fabs(rzd) < 0.001) rzd = 0.0;
             const float len = (float)sqrt(lxy + rzd * rzd * p.dVZ * p.dVZ);
             const float sr = (r & 1) ? sum[r >> 1].y : sum[r >> 1].x;
@@ -543,6 +554,7 @@ SiddonArgs make_args(TigrePlan* P, int a0) {
     a.nX = P->d.nX; a.nY = P->d.nY; a.nZ = P->d.nZ; a.nU = P->d.nU; a.nV = P->d.nV;
     a.dVX = P->d.dVX; a.dVY = P->d.dVY; a.dVZ = P->d.dVZ;
     a.zpad = 1;
+    a.parallel = P->parallel ? 1 : 0;
     a.status = P->d_status;
     return a;
 }

@@ -106,6 +106,7 @@ struct Dims {
 
 struct TigrePlan {
     int device = 0;
+    bool parallel = false;       // parallel-beam geometry (TIGRE_PLAN_PARALLEL)
     tigre::Dims d{};
     std::vector<tigre::FrameSiddon> h_siddon;
     std::vector<tigre::FrameInterp> h_interp;
