@@ -117,6 +117,12 @@ int tigre_voxel_backprojection2(const float* projections, const TigreGeometry* g
 int tigre_pocs_tv(const float* img, float* dst, float alpha, const long* image_size, int max_iter,
                   const int* gpu_ids, int n_gpus);
 
+/* TV denoising by the primal-dual iteration of tvdenoising (Common/CUDA/tv_proximal.hpp,
+ * tv_proximal.cu:185), the operator behind tigre.utilities.im3ddenoise (_tv_proximal.pyx).
+ * src, dst: (nZ, nY, nX) float32 host arrays; image_size = {nX, nY, nZ}; spacing = {dX, dY, dZ}. */
+int tigre_tvdenoising(const float* src, float* dst, float lambda, const float* spacing, const long* image_size,
+                      int max_iter, const int* gpu_ids, int n_gpus);
+
 /* Parallel-beam projection and backprojection.  Replace siddon_ray_projection_parallel
  * (Common/CUDA/Siddon_projection_parallel.hpp, Siddon_projection_parallel.cu:270),
  * interpolation_projection_parallel (ray_interpolated_projection_parallel.hpp,
@@ -189,6 +195,11 @@ int tigre_tv_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha
  * address with that device current; make it before any stream capture. */
 int tigre_tv_pocs_noalloc(void* d_img, int dtype, long nx, long ny, long nz, float alpha, int max_iter,
                           float* d_work, void* stream);
+/* Device TV denoising (same iteration as tigre_tvdenoising) of d_src into d_dst (may alias);
+ * d_work: tigre_tv_denoise_work_floats(nx, ny, nz) floats of caller scratch. */
+long long tigre_tv_denoise_work_floats(long nx, long ny, long nz);
+int tigre_tv_denoise(const float* d_src, float* d_dst, long nx, long ny, long nz, float lambda, const float* spacing,
+                     int max_iter, float* d_work, void* stream);
 /* TV gradient (GD_TV.cu:117-143, single-device boundary rule) into d_grad (FP32). */
 int tigre_tv_gradient(const void* d_img, int dtype, float* d_grad, long nx, long ny, long nz, void* stream);
 /* TV value sum_i |grad f_i| consistent with tigre_tv_gradient; added into *d_out (FP64). */

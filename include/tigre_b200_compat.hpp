@@ -65,5 +65,8 @@ int voxel_backprojection_parallel(float* projections, Geometry geo, float* resul
                                   int nalpha, const GpuIds& gpuids);
 // The reference returns void here; errors are reported on stderr and leave dst unchanged.
 void pocs_tv(float* img, float* dst, float alpha, const long* image_size, int maxIter, const GpuIds& gpuids);
+// Common/CUDA/tv_proximal.hpp:52: TV denoising (im3ddenoise); void like the reference, errors on stderr.
+void tvdenoising(float* src, float* dst, float lambda, const float* spacing, const long* image_size, int maxIter,
+                const GpuIds& gpuids);
 
 #endif  // TIGRE_B200_COMPAT_HPP

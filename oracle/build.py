@@ -32,6 +32,8 @@ REF_GROUPS = {
     "atb": (["TIGRE_common.cpp", "GpuIds.cpp", "gpuUtils.cu", "voxel_backprojection.cu",
              "voxel_backprojection2.cu", "voxel_backprojection_parallel.cu"], "REF_ATB"),
     "tv": (["TIGRE_common.cpp", "GpuIds.cpp", "gpuUtils.cu", "GD_TV.cu"], "REF_TV"),
+    # a separate extension in the reference too (_tv_proximal): it repeats helpers of GD_TV.cu
+    "prox": (["TIGRE_common.cpp", "GpuIds.cpp", "gpuUtils.cu", "tv_proximal.cu"], "REF_PROX"),
 }
 
 

@@ -174,10 +174,11 @@ def pocs_tv(img, alpha, maxiter, nthreads=0):
 
 
 # ---------------------------------------------------------------- FDK pieces --
-def fdk_filter(proj, geo, angles, filter=None):  # noqa: A002
+def fdk_filter(proj, geo, angles, filter=None, cosine=True):  # noqa: A002
     """Cosine weighting + ramp filtering exactly as the reference's host path:
     single_pass_algorithms.py:186-197 then filtering.py:15-53 (scipy.fft on
-    complex64, two projections per transform)."""
+    complex64, two projections per transform).  cosine=False: the ramp filter
+    alone, as fbp uses it (single_pass_algorithms.py:221)."""
     from scipy.fft import fft, ifft
     g = copy.deepcopy(geo)
     g.check_geo(angles)
@@ -187,7 +188,7 @@ def fdk_filter(proj, geo, angles, filter=None):  # noqa: A002
     yv = np.arange(-nv / 2 + 0.5, 1 + nv / 2 - 0.5) * dv
     yy, xx = np.meshgrid(xv, yv)
     dsd, dso = float(g.DSD[0]), float(g.DSO[0])
-    w = dsd / np.sqrt(dsd ** 2 + xx ** 2 + yy ** 2)
+    w = dsd / np.sqrt(dsd ** 2 + xx ** 2 + yy ** 2) if cosine else np.ones_like(xx)
     p = np.multiply(np.asarray(proj, dtype=np.float32), w).astype(np.float32)
 
     def nextpow2(n):
@@ -237,6 +238,135 @@ def fdk_filter(proj, geo, angles, filter=None):  # noqa: A002
 
 def fdk(proj, geo, angles, filter=None):  # noqa: A002
     return atb(fdk_filter(proj, geo, angles, filter), geo, angles, "FDK")
+
+
+def fbp(proj, geo, angles, filter=None):  # noqa: A002
+    """Parallel-beam FBP of single_pass_algorithms.py:206-228: ramp filter, parallel
+    backprojection, times DSO/DSD."""
+    g = copy.deepcopy(geo)
+    g.check_geo(angles)
+    w = float(np.asarray(g.DSO).reshape(-1)[0]) / float(np.asarray(g.DSD).reshape(-1)[0])
+    return (atb(fdk_filter(proj, geo, angles, filter, cosine=False), geo, angles, "FDK") * np.float32(w))
+
+
+def tvdenoise(img, niter, lmbda, spacing=(1.0, 1.0, 1.0)):
+    """TV denoising of tvdenoising (tv_proximal.cu:185-630, one device) in FP64: the image
+    between a lower slice holding image slice 1 and an upper zero slice (cpy_from_host,
+    :672-692), u = f, p = 0, then maxIter steps of update_u (:136-153) and update_p
+    (:156-181) with the reference's FP32 step sizes.  spacing = (dX, dY, dZ)."""
+    img = np.asarray(img, dtype=np.float64)
+    nz = img.shape[0]
+    dxs, dys, dzs = (float(v) for v in spacing)
+    f = np.zeros((nz + 2,) + img.shape[1:], dtype=np.float64)
+    if nz > 1:
+        f[0] = img[1]
+    f[1:nz + 1] = img
+    u = f.copy()
+    pz, py, px = np.zeros_like(u), np.zeros_like(u), np.zeros_like(u)
+    for i in range(int(niter)):
+        tau2 = np.float32(0.3) + np.float32(0.02) * np.float32(i)
+        tau1 = (np.float32(1) / tau2) * (np.float32(1) / np.float32(6) - np.float32(5) / (np.float32(15) + np.float32(i)))
+        tau1, tau2 = float(tau1), float(tau2)
+        div = pz.copy()
+        div[1:] = (pz[1:] - pz[:-1]) / dzs
+        d = py.copy()
+        d[:, 1:] = (py[:, 1:] - py[:, :-1]) / dys
+        div += d
+        d = px.copy()
+        d[:, :, 1:] = (px[:, :, 1:] - px[:, :, :-1]) / dxs
+        div += d
+        u = u * (1.0 - tau1) + tau1 * (f + div / lmbda)
+        gz = np.zeros_like(u); gz[:-1] = (u[1:] - u[:-1]) / dzs
+        gy = np.zeros_like(u); gy[:, :-1] = (u[:, 1:] - u[:, :-1]) / dys
+        gx = np.zeros_like(u); gx[:, :, :-1] = (u[:, :, 1:] - u[:, :, :-1]) / dxs
+        qz, qy, qx = pz + tau2 * gz, py + tau2 * gy, px + tau2 * gx
+        nrm = np.maximum(1.0, np.sqrt(qz * qz + qy * qy + qx * qx))
+        pz, py, px = qz / nrm, qy / nrm, qx / nrm
+    return u[1:nz + 1].astype(np.float32)
+
+
+def im3ddenoise(img, niter=50, lmbda=15.0):
+    """im_3d_denoise.py:7-27 over the oracle tvdenoise (min/max scaling)."""
+    img = np.asarray(img, dtype=np.float32)
+    lo = img.min()
+    x = img - lo
+    hi = x.max()
+    x = x / hi
+    return (tvdenoise(x, niter, lmbda) * hi + lo).astype(np.float32)
+
+
+def fista(proj, geo, angles, niter, hyper, tviter=20, tvlambda=0.1):
+    """FISTA of ista_algorithms.py:13-176 in FP64 over the oracle pair and oracle im3ddenoise."""
+    b = np.asarray(proj, dtype=np.float64)
+    x = np.zeros(tuple(int(v) for v in geo.nVoxel), dtype=np.float64)
+    bm = 1.0 / hyper
+    x_rec = x.copy()
+    lam = 2.0 * bm * tvlambda
+    t = 1.0
+    for _ in range(niter):
+        r = b - ax(x.astype(np.float32), geo, angles, "interpolated")
+        x = np.maximum(x + 2.0 * bm * atb(r.astype(np.float32), geo, angles, "matched"), 0.0)
+        x_old = x_rec
+        x_rec = im3ddenoise(x.astype(np.float32), tviter, 1.0 / lam).astype(np.float64)
+        t_old = t
+        t = (1.0 + np.sqrt(1.0 + 4.0 * t * t)) / 2.0
+        x = x_rec + (t_old - 1.0) / t * (x_rec - x_old)
+    return x.astype(np.float32)
+
+
+def lsqr(proj, geo, angles, niter):
+    """LSQR of krylov_subspace_algorithms.py:101-187 with FP64 vectors over the oracle pair."""
+    A = lambda v: ax(v.astype(np.float32), geo, angles, "Siddon").astype(np.float64)  # noqa: E731
+    At = lambda r: atb(r.astype(np.float32), geo, angles, "matched").astype(np.float64)  # noqa: E731
+    b = np.asarray(proj, dtype=np.float64)
+    x = np.zeros(tuple(int(v) for v in geo.nVoxel), dtype=np.float64)
+    u = b.copy(); beta = np.linalg.norm(u); u /= beta; phibar = beta
+    v = At(u); alpha = np.linalg.norm(v); v /= alpha; rhobar = alpha; w = v.copy()
+    res = []
+    for _ in range(niter):
+        u = A(v) - alpha * u; beta = np.linalg.norm(u); u /= beta
+        v = At(u) - beta * v; alpha = np.linalg.norm(v); v /= alpha
+        rho = np.hypot(rhobar, beta); c, s = rhobar / rho, beta / rho
+        theta = s * alpha; rhobar = -c * alpha; phi = c * phibar; phibar = s * phibar
+        x += (phi / rho) * w; w_old = w; w = v - (theta / rho) * w
+        rn = np.linalg.norm(b - A(x))
+        if res and rn > res[-1]:
+            x -= (phi / rho) * w_old
+            break
+        res.append(rn)
+    return x.astype(np.float32), np.asarray(res)
+
+
+def lsmr(proj, geo, angles, niter, lmbda=1.0):
+    """LSMR of krylov_subspace_algorithms.py:299-439 with FP64 vectors over the oracle pair."""
+    A = lambda v: ax(v.astype(np.float32), geo, angles, "Siddon").astype(np.float64)  # noqa: E731
+    At = lambda r: atb(r.astype(np.float32), geo, angles, "matched").astype(np.float64)  # noqa: E731
+    b = np.asarray(proj, dtype=np.float64)
+    x = np.zeros(tuple(int(v) for v in geo.nVoxel), dtype=np.float64)
+    u = b.copy(); beta = np.linalg.norm(u); u /= beta
+    v = At(u); alpha = np.linalg.norm(v); v /= alpha
+    alphabar, zetabar, rho, rhobar, cbar, sbar = alpha, alpha * beta, 1.0, 1.0, 1.0, 0.0
+    h = v.copy(); hbar = np.zeros_like(h)
+    res = []
+    for _ in range(niter):
+        u = A(v) - alpha * u; beta = np.linalg.norm(u); u /= beta
+        v = At(u) - beta * v; alpha = np.linalg.norm(v); v /= alpha
+        alphahat = np.hypot(alphabar, lmbda)
+        rhopre = rho; rho = np.hypot(alphahat, beta); c, s = alphahat / rho, beta / rho
+        theta = s * alpha; alphabar = c * alpha
+        thetabar = sbar * rho; rhobarpre = rhobar; rhobar = np.hypot(cbar * rho, theta)
+        cbar = cbar * rho / rhobar; sbar = theta / rhobar
+        zeta = cbar * zetabar; zetabar = -sbar * zetabar
+        hbar = h - (thetabar * rho / (rhopre * rhobarpre)) * hbar
+        step = zeta / (rho * rhobar)
+        x += step * hbar
+        h = v - (theta / rho) * h
+        rn = np.linalg.norm(b - A(x))
+        if res and rn > res[-1]:
+            x -= step * hbar
+            break
+        res.append(rn)
+    return x.astype(np.float32), np.asarray(res)
 
 
 def cgls(proj, geo, angles, niter):

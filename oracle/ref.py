@@ -45,7 +45,7 @@ class Geometry(C.Structure):
 
 
 def available() -> bool:
-    return all(os.path.exists(os.path.join(REF_DIR, "libref_%s.so" % g)) for g in ("ax", "atb", "tv"))
+    return all(os.path.exists(os.path.join(REF_DIR, "libref_%s.so" % g)) for g in ("ax", "atb", "tv", "prox"))
 
 
 def _geo_dict(geo, angles):
@@ -135,6 +135,16 @@ def _worker(spec_path):
             L.ref_pocs_tv(inp.ctypes.data, out.ctypes.data, float(spec["alpha"]), C.cast(size, C.c_void_p),
                           int(spec["maxiter"]), dev)
             times.append(time.perf_counter() - t)
+    elif op == "tvdenoise":
+        L = C.CDLL(os.path.join(REF_DIR, "libref_prox.so"))
+        L.ref_tvdenoise.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_int, C.c_int]
+        out = np.empty_like(inp)
+        size = (C.c_long * 3)(inp.shape[2], inp.shape[1], inp.shape[0])
+        for _ in range(int(spec.get("repeat", 1))):
+            t = time.perf_counter()
+            L.ref_tvdenoise(inp.ctypes.data, out.ctypes.data, float(spec["lmbda"]), C.cast(size, C.c_void_p),
+                            int(spec["maxiter"]), dev)
+            times.append(time.perf_counter() - t)
     else:
         raise SystemExit("unknown op " + op)
     np.save(spec["output"], out)
@@ -182,3 +192,8 @@ if __name__ == "__main__":
         _worker(sys.argv[2])
     else:
         print(__doc__)
+
+
+def tvdenoise(img, lmbda, maxiter, repeat=1, device=0):
+    """The reference's tvdenoising on img (already scaled as im3ddenoise scales it)."""
+    return _run("tvdenoise", img, lmbda=float(lmbda), maxiter=int(maxiter), repeat=repeat, device=device)

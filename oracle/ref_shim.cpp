@@ -24,6 +24,8 @@
 #include "voxel_backprojection_parallel.hpp"
 #elif defined(REF_TV)
 #include "GD_TV.hpp"
+#elif defined(REF_PROX)
+#include "tv_proximal.hpp"
 #endif
 
 namespace {
@@ -73,6 +75,14 @@ int ref_atb(float* proj, const Geometry* geo, float* out, const float* angles, i
 int ref_pocs_tv(float* img, float* dst, float alpha, const long* image_size, int maxiter, int dev) {
     OneGpu g(dev);
     pocs_tv(img, dst, alpha, image_size, maxiter, g.ids);
+    return 0;
+}
+#elif defined(REF_PROX)
+// tvdenoising (tv_proximal.cu:185) with unit spacing, as _tv_proximal.pyx:52-55 passes it.
+int ref_tvdenoise(float* img, float* dst, float lambda, const long* image_size, int maxiter, int dev) {
+    OneGpu g(dev);
+    const float spacing[3] = {1.f, 1.f, 1.f};
+    tvdenoising(img, dst, lambda, spacing, image_size, maxiter, g.ids);
     return 0;
 }
 #endif

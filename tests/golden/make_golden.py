@@ -32,6 +32,8 @@ def main():
         res["fdk"], _ = ref.atb(res["siddon"], geo, ang, "FDK")
         res["matched"], _ = ref.atb(res["siddon"], geo, ang, "matched")
         res["pocs_tv"], _ = ref.pocs_tv(img, GC.TV_ALPHA, GC.TV_ITERS)
+        scaled = (img - img.min()) / (img - img.min()).max()
+        res["tvdenoise"], _ = ref.tvdenoise(scaled.astype(np.float32), GC.DENOISE_LAMBDA, GC.DENOISE_ITERS)
         np.savez_compressed(os.path.join(out_dir, "ref_%s.npz" % name), **res)
         print(name, {k: v.shape for k, v in res.items()})
 

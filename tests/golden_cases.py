@@ -6,6 +6,8 @@ from tigre_b200.utilities.phantom import random_ellipsoids
 
 TV_ALPHA = 0.002
 TV_ITERS = 10
+DENOISE_LAMBDA = 15.0
+DENOISE_ITERS = 30
 
 CASES = ("small", "offsets", "parallel")
 

@@ -25,6 +25,7 @@ TOLS = {
     "fdk": (2e-3, 2e-4),
     "matched": (2e-3, 2e-4),
     "pocs_tv": (1e-5, 1e-6),
+    "tvdenoise": (1e-5, 1e-6),
 }
 
 
@@ -39,6 +40,7 @@ def test_oracle_matches_reference_cuda(name):
         "fdk": O.atb(ref["siddon"], geo, ang, "FDK"),
         "matched": O.atb(ref["siddon"], geo, ang, "matched"),
         "pocs_tv": O.pocs_tv(img, GC.TV_ALPHA, GC.TV_ITERS),
+        "tvdenoise": O.tvdenoise((img - img.min()) / (img - img.min()).max(), GC.DENOISE_ITERS, GC.DENOISE_LAMBDA),
     }
     for k, (tmax, tl2) in TOLS.items():
         mx, l2 = rel_err(got[k], ref[k])

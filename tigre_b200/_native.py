@@ -89,6 +89,11 @@ _SIGS = {
                                 C.c_void_p]),
     "tigre_tv_pocs_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_int,
                                         C.c_void_p, C.c_void_p]),
+    "tigre_tvdenoising": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                    C.c_int]),
+    "tigre_tv_denoise_work_floats": (C.c_longlong, [C.c_long, C.c_long, C.c_long]),
+    "tigre_tv_denoise": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long, C.c_long, C.c_long, C.c_float, C.c_void_p,
+                                   C.c_int, C.c_void_p, C.c_void_p]),
     "tigre_tv_gradient": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_long, C.c_long, C.c_long, C.c_void_p]),
     "tigre_tv_value": (C.c_int, [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_long, C.c_void_p, C.c_void_p]),
     "tigre_sumsq": (C.c_int, [C.c_void_p, C.c_int, C.c_long, C.c_void_p, C.c_void_p]),

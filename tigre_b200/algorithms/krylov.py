@@ -1,4 +1,4 @@
-"""CGLS, device-resident.
+"""Krylov solvers (CGLS, LSQR, LSMR), device-resident.
 
 Same iteration and outputs as the reference (Python/tigre/algorithms/
 krylov_subspace_algorithms.py:22-99): Siddon forward projection, matched
@@ -130,3 +130,141 @@ def cgls(proj, geo, angles, niter, **kwargs):
     if kwargs.get("computel2", False) or kwargs.get("return_residuals", False):
         return out, l2.reshape(1, -1).astype(np.float32)
     return out
+
+
+def _norm(t):
+    """FP64 2-norm of a device tensor (FP64 accumulation kernel)."""
+    return float(P.sumsq(t).sqrt().item())
+
+
+def _residual(prob, x):
+    return _norm(prob.b - P.ax(x, prob.plan, "Siddon"))
+
+
+def lsqr_device(prob: Problem, niter, x0=None, verbose=False):
+    """LSQR of krylov_subspace_algorithms.py:101-187 (Paige & Saunders): Siddon / matched pair,
+    vectors resident on the device, scalar recurrences in FP64 on the host.  The logged
+    residual is the explicit |b - A x| of the reference (:174); when it grows, the last step is
+    undone and the iteration stops (:175-187)."""
+    T = torch()
+    plan = prob.plan
+    x = prob.zeros_vol() if x0 is None else prob.to_device_vol(x0)
+    u = prob.b - P.ax(x, plan, "Siddon")
+    beta = _norm(u)
+    u.div_(beta)
+    phibar = beta
+    v = P.atb(u, plan, "matched")
+    alpha = _norm(v)
+    v.div_(alpha)
+    rhobar = alpha
+    w = v.clone()
+    tmp_p = T.empty_like(u)
+    tmp_v = T.empty_like(v)
+    l2 = []
+    for it in range(niter):
+        P.ax(v, plan, "Siddon", out=tmp_p)
+        u = tmp_p - alpha * u
+        beta = _norm(u)
+        u.div_(beta)
+        P.atb(u, plan, "matched", out=tmp_v)
+        v = tmp_v - beta * v
+        alpha = _norm(v)
+        v.div_(alpha)
+        rho = float(np.hypot(rhobar, beta))
+        c, s = rhobar / rho, beta / rho
+        theta = s * alpha
+        rhobar = -c * alpha
+        phi = c * phibar
+        phibar = s * phibar
+        w_old = w
+        x.add_(w_old, alpha=phi / rho)
+        w = v - (theta / rho) * w_old
+        res = _residual(prob, x)
+        if it > 0 and res > l2[-1]:
+            x.add_(w_old, alpha=-phi / rho)
+            if verbose:
+                print("LSQR exited due to divergence at iteration", it)
+            break
+        l2.append(res)
+    return x, np.asarray(l2, dtype=np.float64)
+
+
+def lsmr_device(prob: Problem, niter, x0=None, lmbda=1.0, verbose=False):
+    """LSMR of krylov_subspace_algorithms.py:299-439 (Fong & Saunders) with damping lmbda (the
+    reference passes its generic lmbda, default 1).  Same pair, residual log and divergence
+    rule as lsqr_device."""
+    plan = prob.plan
+    x = prob.zeros_vol() if x0 is None else prob.to_device_vol(x0)
+    u = prob.b - P.ax(x, plan, "Siddon")
+    beta = _norm(u)
+    u.div_(beta)
+    v = P.atb(u, plan, "matched")
+    alpha = _norm(v)
+    v.div_(alpha)
+    alphabar, zetabar = alpha, alpha * beta
+    rho, rhobar, cbar, sbar = 1.0, 1.0, 1.0, 0.0
+    h = v.clone()
+    hbar = None
+    zeta = 0.0
+    l2 = []
+    for it in range(niter):
+        u = P.ax(v, plan, "Siddon") - alpha * u
+        beta = _norm(u)
+        u.div_(beta)
+        v = P.atb(u, plan, "matched") - beta * v
+        alpha = _norm(v)
+        v.div_(alpha)
+        alphahat = float(np.hypot(alphabar, lmbda))
+        rhopre = rho
+        rho = float(np.hypot(alphahat, beta))
+        c, s = alphahat / rho, beta / rho
+        theta = s * alpha
+        alphabar = c * alpha
+        thetabar = sbar * rho
+        rhobarpre = rhobar
+        rhobar = float(np.hypot(cbar * rho, theta))
+        cbar = cbar * rho / rhobar
+        sbar = theta / rhobar
+        zeta = cbar * zetabar
+        zetabar = -sbar * zetabar
+        hbar = h.clone() if hbar is None else h - (thetabar * rho / (rhopre * rhobarpre)) * hbar
+        step = zeta / (rho * rhobar)
+        x.add_(hbar, alpha=step)
+        h = v - (theta / rho) * h
+        res = _residual(prob, x)
+        if it > 0 and res > l2[-1]:
+            x.add_(hbar, alpha=-step)
+            if verbose:
+                print("LSMR exited due to divergence at iteration", it)
+            break
+        l2.append(res)
+    return x, np.asarray(l2, dtype=np.float64)
+
+
+def _krylov_entry(solver, proj, geo, angles, niter, kwargs, **extra):
+    prob = Problem(proj, geo, angles, kwargs.get("gpuids"))
+    init = kwargs.get("init", None)
+    x0 = None
+    if isinstance(init, str):
+        if init == "FDK":
+            from .single_pass import fdk_device
+            x0 = fdk_device(prob).clamp_(min=0)
+        elif init != "none":
+            raise ValueError("wrong value for initialization")
+    elif init is not None:
+        x0 = init
+    x, l2 = solver(prob, niter, x0=x0, verbose=kwargs.get("verbose", False), **extra)
+    out = prob.out(x)
+    if kwargs.get("computel2", False):
+        return out, l2.reshape(1, -1).astype(np.float32)
+    return out
+
+
+def lsqr(proj, geo, angles, niter, **kwargs):
+    """Drop-in for tigre.algorithms.lsqr(proj, geo, angles, niter, init=, computel2=, gpuids=, verbose=)."""
+    return _krylov_entry(lsqr_device, proj, geo, angles, niter, kwargs)
+
+
+def lsmr(proj, geo, angles, niter, **kwargs):
+    """Drop-in for tigre.algorithms.lsmr(proj, geo, angles, niter, lmbda=, init=, computel2=, gpuids=, verbose=)."""
+    return _krylov_entry(lsmr_device, proj, geo, angles, niter, kwargs, lmbda=float(kwargs.get("lmbda", 1.0)))

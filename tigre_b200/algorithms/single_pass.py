@@ -90,6 +90,13 @@ fdk = FDK
 
 
 def fbp(proj, geo, angles, **kwargs):
+    """Parallel-beam FBP, drop-in for tigre.algorithms.fbp (single_pass_algorithms.py:206-228):
+    ramp filter on the device, parallel backprojection, times DSO/DSD."""
     if getattr(geo, "mode", "cone") != "parallel":
         raise ValueError("Only use FBP for parallel beam. Check geo.mode.")
-    raise NotImplementedError("parallel-beam projectors are not part of tigre_b200")
+    prob = Problem(proj, geo, angles, kwargs.get("gpuids"))
+    g = prob.geo
+    filt = F.filter_projections(prob.b, g, prob.n, kwargs.get("filter", None))
+    vol = P.atb(filt, prob.plan, "FDK")
+    vol *= float(np.asarray(g.DSO).reshape(-1)[0]) / float(np.asarray(g.DSD).reshape(-1)[0])
+    return prob.out(vol)

@@ -376,6 +376,30 @@ int host_pocs_tv(const float* img, float* dst, float alpha, const long* image_si
     return TIGRE_SUCCESS;
 }
 
+int host_tvdenoising(const float* src, float* dst, float lambda, const float* spacing, const long* image_size,
+                     int max_iter, const int* ids, int n) {
+    if (!src || !dst || !image_size) return fail(TIGRE_ERR_BAD_ASSERT, "null argument");
+    const long nx = image_size[0], ny = image_size[1], nz = image_size[2];
+    if (nx <= 0 || ny <= 0 || nz <= 0) return fail(TIGRE_ERR_BAD_ASSERT, "bad image size");
+    int dev = 0;
+    if (int rc = pick_device(ids, n, &dev)) return rc;
+    DeviceGuard g(dev);
+    DeviceState* S = state(dev);
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (int rc = S->init(dev)) return rc;
+    const size_t nvox = (size_t)nx * ny * nz;
+    void *dimg = nullptr, *dwork = nullptr;
+    if (int rc = S->get(0, nvox * sizeof(float), &dimg)) return rc;
+    if (int rc = S->get(1, (size_t)tigre_tv_denoise_work_floats(nx, ny, nz) * sizeof(float), &dwork)) return rc;
+    TIGRE_CUDA(cudaMemcpyAsync(dimg, src, nvox * sizeof(float), cudaMemcpyHostToDevice, S->st));
+    if (int rc = tigre_tv_denoise((const float*)dimg, (float*)dimg, nx, ny, nz, lambda, spacing, max_iter,
+                                  (float*)dwork, S->st))
+        return rc;
+    TIGRE_CUDA(cudaMemcpyAsync(dst, dimg, nvox * sizeof(float), cudaMemcpyDeviceToHost, S->st));
+    TIGRE_CUDA(cudaStreamSynchronize(S->st));
+    return TIGRE_SUCCESS;
+}
+
 }  // namespace
 
 extern "C" void tigre_release_cache(void) {
@@ -413,6 +437,11 @@ int tigre_voxel_backprojection2(const float* proj, const TigreGeometry* geo, flo
 int tigre_pocs_tv(const float* img, float* dst, float alpha, const long* image_size, int max_iter, const int* ids,
                   int n) {
     return host_pocs_tv(img, dst, alpha, image_size, max_iter, ids, n);
+}
+
+int tigre_tvdenoising(const float* src, float* dst, float lambda, const float* spacing, const long* image_size,
+                      int max_iter, const int* ids, int n) {
+    return host_tvdenoising(src, dst, lambda, spacing, image_size, max_iter, ids, n);
 }
 
 int tigre_siddon_ray_projection_parallel(const float* img, const TigreGeometry* geo, float* const* result,

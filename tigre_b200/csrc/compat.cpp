@@ -55,3 +55,9 @@ void pocs_tv(float* img, float* dst, float alpha, const long* image_size, int ma
     const int rc = tigre_pocs_tv(img, dst, alpha, image_size, maxIter, ids.m_piDeviceIds, ids.m_iCount);
     if (rc) std::fprintf(stderr, "minimizeTV:POCS_TV: error %d: %s\n", rc, tigre_last_error());
 }
+
+void tvdenoising(float* src, float* dst, float lambda, const float* spacing, const long* image_size, int maxIter,
+                 const GpuIds& ids) {
+    const int rc = tigre_tvdenoising(src, dst, lambda, spacing, image_size, maxIter, ids.m_piDeviceIds, ids.m_iCount);
+    if (rc) std::fprintf(stderr, "tvdenoising failed with code %d: %s\n", rc, tigre_last_error());
+}
