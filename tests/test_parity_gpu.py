@@ -424,3 +424,20 @@ def test_tv_denoise_matches_oracle():
         out = tv_denoise_device(torch.from_numpy(x).cuda(), 10, 5.0).cpu().numpy()
         mx, l2 = G.rel_err(out, O.tvdenoise(x, 10, 5.0))
         assert mx <= TOL and l2 <= TOL, (nz, mx, l2)
+
+
+@pytest.mark.parametrize("nv", [300, 520])
+def test_siddon_tall_detectors(nv):
+    """Tall detectors select 4 (nV >= 256) or 8 (nV >= 512) rows per thread in the
+    cell-interval kernel; partial row tiles included."""
+    torch = _torch()
+    from tigre_b200 import _native as N, projectors as P
+    from tigre_b200.utilities.geometry import cone_geometry
+    geo = cone_geometry((40, 36, 36), (40.0, 36.0, 36.0), (nv, 28), (0.1, 1.6))
+    ang = G.angles(5)
+    img = G.phantom((40, 36, 36), seed=14)
+    plan = N.get_plan(N.checked_geometry(geo, ang), 0)
+    got = P.ax(torch.from_numpy(img).cuda(), plan, "Siddon").cpu().numpy()
+    mx, l2 = G.rel_err(got, O.ax(img, geo, ang, "Siddon"))
+    assert mx <= TOL and l2 <= TOL, (nv, mx, l2)
+    assert plan.status() == 0

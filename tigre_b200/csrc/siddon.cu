@@ -388,7 +388,7 @@ __device__ __forceinline__ float ldz(uintptr_t cb, float t) {
 }
 
 template <typename TV, typename TP, int R>
-__global__ void __launch_bounds__(128, 6) siddon_cells_kernel(SiddonArgs p) {
+__global__ void __launch_bounds__(128, R >= 8 ? 4 : 6) siddon_cells_kernel(SiddonArgs p) {
     static_assert(R % 2 == 0, "rows are processed in pairs");
     constexpr int H = R / 2;
     const int lane = threadIdx.x & 31;
@@ -636,7 +636,8 @@ int launch_siddon_columns(TigrePlan* P, const void* vol_z, int vdt, void* proj, 
 
 template <typename TV, typename TP>
 static void launch_cells_typed(const SiddonArgs& a, int rows_per_thread, dim3 grid, cudaStream_t st) {
-    if (rows_per_thread == 4) siddon_cells_kernel<TV, TP, 4><<<grid, 128, 0, st>>>(a);
+    if (rows_per_thread == 8) siddon_cells_kernel<TV, TP, 8><<<grid, 128, 0, st>>>(a);
+    else if (rows_per_thread == 4) siddon_cells_kernel<TV, TP, 4><<<grid, 128, 0, st>>>(a);
     else siddon_cells_kernel<TV, TP, 2><<<grid, 128, 0, st>>>(a);
 }
 
@@ -647,7 +648,8 @@ int launch_siddon_cells(TigrePlan* P, const void* vol_z, int vdt, void* proj, in
     a.proj = proj;
     a.zpad = P->cells_zpad;
     const int nv = P->d.nV;
-    const int R = nv >= 256 ? 4 : 2;
+    // rows per thread: 8 (256 rows per warp, 4 resident blocks per SM) for tall detectors
+    const int R = nv >= 512 ? 8 : (nv >= 256 ? 4 : 2);
     const int na = a1 - a0;
     for (int c = 0; c < na; c += 65535) {
         SiddonArgs ac = a;
