@@ -161,6 +161,11 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs p) {
         const float2 q0f2 = pk2(q0f), q0o2 = pk2(q0o), q0z2 = pk2(q0z);
         float2 kk = pk2(0.f, 1.f);
         float sa = 0.f, sb = 0.f;
+        // Consecutive samples are a fraction of a voxel apart and often share their trilinear
+        // cell: the corner quads of the previous sample are kept and reloaded only when the
+        // cell index changes (a lane that skips a load adds no L1 traffic).
+        uint32_t pidx = 0xffffffffu;
+        float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0;
         int k = 0;
 #pragma unroll 1
         for (; k + 1 < nsamp; k += 2) {
@@ -175,10 +180,17 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs p) {
             const float2 fz = __ffma2_rn(__fadd2_rn(tz, pk2(-M)), pk2(-1.f), qz);
             const uint32_t ia = __float_as_uint(tf.x) + __float_as_uint(to.x) * FP + __float_as_uint(tz.x) * PL + bias;
             const uint32_t ib = __float_as_uint(tf.y) + __float_as_uint(to.y) * FP + __float_as_uint(tz.y) * PL + bias;
-            const float4 a0 = ldq<TV>(quads, ia), a1 = ldq<TV>(quads, ia + FP);
-            const float4 b0 = ldq<TV>(quads, ib), b1 = ldq<TV>(quads, ib + FP);
-            sa += tri(a0, a1, ff.x, fz.x, fo.x);
-            sb += tri(b0, b1, ff.y, fz.y, fo.y);
+            if (ia != pidx) {
+                p0 = ldq<TV>(quads, ia);
+                p1 = ldq<TV>(quads, ia + FP);
+            }
+            sa += tri(p0, p1, ff.x, fz.x, fo.x);
+            if (ib != ia) {
+                p0 = ldq<TV>(quads, ib);
+                p1 = ldq<TV>(quads, ib + FP);
+            }
+            sb += tri(p0, p1, ff.y, fz.y, fo.y);
+            pidx = ib;
         }
         sum = sa + sb;
         if (k < nsamp) {   // odd count: last sample
