@@ -11,6 +11,7 @@
 //                     Common/CUDA/voxel_backprojection.cu:762-898
 // The reference evaluates most of them in float; here everything is double.
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -241,6 +242,70 @@ void parallel_frames(const TigreGeometry* g, const Dims& d, int i, double al, do
     fb.offu = (float)offu; fb.offv = (float)offv;
 }
 
+// Shared-memory wavefronts of the staged backprojector's four bilinear taps for a float patch
+// of row pitch BU words, estimated on sample blocks, views and slices with the kernel's own
+// thread layout (a warp = 8 x 4 voxel columns) and patch origin rule.  A warp load costs as
+// many wavefronts as the largest number of distinct words that fall in one bank.
+double bp_bank_cost(const TigrePlan* plan, int BU, int bx, int bz) {
+    const Dims& d = plan->d;
+    const int na = (int)plan->h_bpk.size();
+    const int vstep_views = std::max(1, na / 24);
+    const int nbx = (d.nX + bx - 1) / bx, nby = (d.nY + bx - 1) / bx, nbz = (d.nZ + bz - 1) / bz;
+    const int sbx[3] = {0, nbx / 2, nbx - 1}, sby[3] = {0, nby / 2, nby - 1}, sbz[2] = {0, nbz / 2};
+    const int warps[2] = {0, 5};
+    const int slices[4] = {0, bz / 3, (2 * bz) / 3, bz - 1};
+    double cost = 0.0;
+    for (int a = 0; a < na; a += vstep_views) {
+        const FrameBPK& k = plan->h_bpk[a];
+        auto proj = [&](double x, double y, double z, double& u, double& v) {
+            const double vx = k.b[0] + x * k.dx[0] + y * k.dy[0] + z * k.dz[0];
+            const double vy = k.b[1] + x * k.dx[1] + y * k.dy[1] + z * k.dz[1];
+            const double vz = k.b[2] + x * k.dx[2] + y * k.dy[2] + z * k.dz[2];
+            const double t = (double)k.tnum / vx;
+            u = vy * t + k.cu - 0.5;
+            v = vz * t + k.cv - 0.5;
+        };
+        for (int ix : sbx)
+            for (int iy : sby)
+                for (int iz : sbz) {
+                    const int x0 = ix * bx, y0 = iy * bx, z0 = iz * bz;
+                    double umin = 1e300, vmin = 1e300;
+                    for (int c = 0; c < 8; ++c) {
+                        double u, v;
+                        proj(std::min(x0 + ((c & 1) ? bx - 1 : 0), d.nX - 1), std::min(y0 + ((c & 2) ? bx - 1 : 0), d.nY - 1),
+                             std::min(z0 + ((c & 4) ? bz - 1 : 0), d.nZ - 1), u, v);
+                        umin = std::min(umin, u);
+                        vmin = std::min(vmin, v);
+                    }
+                    if (!std::isfinite(umin) || !std::isfinite(vmin)) continue;
+                    int u0 = (int)std::floor(umin) - 1;
+                    u0 = u0 >= 0 ? (u0 / 4) * 4 : -(((-u0) + 3) / 4) * 4;
+                    const int v0 = (int)std::floor(vmin) - 1;
+                    for (int w : warps)
+                        for (int ks : slices) {
+                            long words[4][32];
+                            for (int ln = 0; ln < 32; ++ln) {
+                                const int x = x0 + (w & 1) * 8 + (ln & 7), y = y0 + (w >> 1) * 4 + (ln >> 3);
+                                double u, v;
+                                proj(std::min(x, d.nX - 1), std::min(y, d.nY - 1), std::min(z0 + ks, d.nZ - 1), u, v);
+                                const long iu = (long)std::floor(u - u0), iv = (long)std::floor(v - v0);
+                                const long base = iv * BU + iu;
+                                words[0][ln] = base; words[1][ln] = base + 1;
+                                words[2][ln] = base + BU; words[3][ln] = base + BU + 1;
+                            }
+                            for (auto& tap : words) {
+                                int per_bank[32] = {0};
+                                std::sort(tap, tap + 32);
+                                for (int ln = 0; ln < 32; ++ln)
+                                    if (ln == 0 || tap[ln] != tap[ln - 1]) ++per_bank[((tap[ln] % 32) + 32) % 32];
+                                cost += *std::max_element(per_bank, per_bank + 32);
+                            }
+                        }
+                }
+    }
+    return cost;
+}
+
 int compute_frames(const TigreGeometry* g, const float* angles, int nangles, TigrePlan* plan) {
     TIGRE_CHECK(g != nullptr && angles != nullptr, "null geometry or angles");
     TIGRE_CHECK(nangles > 0, "nangles must be positive");
@@ -443,16 +508,31 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
                 }
     }
     {
-        // Row pitch of the patch in 4-byte banks: = 4 (mod 8), so 8 neighbouring rows start in
-        // 8 distinct bank quads and the 4 taps of up to 8 rows x 4 columns per warp load do not
-        // collide.  The TMA box's row must be a multiple of 16 bytes: 4 floats, 8 halves.
+        // Patch box.  The TMA box's row must be a multiple of 16 bytes: 4 floats, 8 halves.
         const int need = (int)std::ceil(ext_u) + 13;
-        int BU = (std::max(need, 4) + 3) / 4 * 4;
-        while (BU % 8 != 4) BU += 4;                  // float rows: BU words
-        int BU16 = (std::max(need, 8) + 7) / 8 * 8;
-        while (BU16 % 16 != 8) BU16 += 8;             // 16-bit rows: BU16 / 2 words
         int BV = (int)std::ceil(ext_v) + 6;
         if (BV < 4) BV = 4;
+        // float rows: the pitch (mod 32 words) with the fewest estimated shared-memory wavefronts
+        // among those whose double buffer fits the 96 KB budget (tuning hook: force one residue)
+        const int base = (std::max(need, 4) + 3) / 4 * 4;
+        int BU = base;
+        while (BU % 8 != 4) BU += 4;
+        int forced = -1;
+        if (const char* pm = std::getenv("TIGRE_B200_BP_PITCH_MOD32")) {
+            const int v = std::atoi(pm);
+            if (v >= 0 && v < 32 && v % 4 == 0) forced = v;
+        }
+        double best = -1.0;
+        for (int r = 0; r < 32; r += 4) {
+            if (forced >= 0 && r != forced) continue;
+            int bu = base;
+            while (bu % 32 != r) bu += 4;
+            if (2.0 * bu * BV * 4 > 96.0 * 1024) continue;
+            const double c = bp_bank_cost(plan, bu, bx, bz);
+            if (best < 0.0 || c < best || (c == best && bu < BU)) { best = c; BU = bu; }
+        }
+        int BU16 = (std::max(need, 8) + 7) / 8 * 8;
+        while (BU16 % 16 != 8) BU16 += 8;             // 16-bit rows: BU16 / 2 words
         if (const char* ov = std::getenv("TIGRE_B200_BP_BOX")) {   // test hook: force a box (e.g. "8x4")
             int bu = 0, bv = 0;
             if (std::sscanf(ov, "%dx%d", &bu, &bv) == 2 && bu > 0 && bv > 0) {
