@@ -242,11 +242,11 @@ void parallel_frames(const TigreGeometry* g, const Dims& d, int i, double al, do
     fb.offu = (float)offu; fb.offv = (float)offv;
 }
 
-// Shared-memory wavefronts of the staged backprojector's four bilinear taps for a float patch
-// of row pitch BU words, estimated on sample blocks, views and slices with the kernel's own
+// Shared-memory wavefronts of the staged backprojector's four bilinear taps for a patch of
+// es-byte texels and row pitch BU texels, estimated on sample blocks, views and slices with the kernel's own
 // thread layout (a warp = 8 x 4 voxel columns) and patch origin rule.  A warp load costs as
 // many wavefronts as the largest number of distinct words that fall in one bank.
-double bp_bank_cost(const TigrePlan* plan, int BU, int bx, int bz) {
+double bp_bank_cost(const TigrePlan* plan, int BU, int es, int bx, int bz) {
     const Dims& d = plan->d;
     const int na = (int)plan->h_bpk.size();
     const int vstep_views = std::max(1, na / 24);
@@ -279,7 +279,8 @@ double bp_bank_cost(const TigrePlan* plan, int BU, int bx, int bz) {
                     }
                     if (!std::isfinite(umin) || !std::isfinite(vmin)) continue;
                     int u0 = (int)std::floor(umin) - 1;
-                    u0 = u0 >= 0 ? (u0 / 4) * 4 : -(((-u0) + 3) / 4) * 4;
+                    const int al = 16 / es;   // TMA: the patch origin's x is 16-byte aligned
+                    u0 = u0 >= 0 ? (u0 / al) * al : -(((-u0) + al - 1) / al) * al;
                     const int v0 = (int)std::floor(vmin) - 1;
                     for (int w : warps)
                         for (int ks : slices) {
@@ -290,8 +291,8 @@ double bp_bank_cost(const TigrePlan* plan, int BU, int bx, int bz) {
                                 proj(std::min(x, d.nX - 1), std::min(y, d.nY - 1), std::min(z0 + ks, d.nZ - 1), u, v);
                                 const long iu = (long)std::floor(u - u0), iv = (long)std::floor(v - v0);
                                 const long base = iv * BU + iu;
-                                words[0][ln] = base; words[1][ln] = base + 1;
-                                words[2][ln] = base + BU; words[3][ln] = base + BU + 1;
+                                words[0][ln] = base * es / 4; words[1][ln] = (base + 1) * es / 4;
+                                words[2][ln] = (base + BU) * es / 4; words[3][ln] = (base + BU + 1) * es / 4;
                             }
                             for (auto& tap : words) {
                                 int per_bank[32] = {0};
@@ -527,12 +528,22 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
             if (forced >= 0 && r != forced) continue;
             int bu = base;
             while (bu % 32 != r) bu += 4;
-            if (2.0 * bu * BV * 4 > 96.0 * 1024) continue;
-            const double c = bp_bank_cost(plan, bu, bx, bz);
+            if (bu > 256 || 2.0 * bu * BV * 4 > 96.0 * 1024) continue;
+            const double c = bp_bank_cost(plan, bu, 4, bx, bz);
             if (best < 0.0 || c < best || (c == best && bu < BU)) { best = c; BU = bu; }
         }
-        int BU16 = (std::max(need, 8) + 7) / 8 * 8;
-        while (BU16 % 16 != 8) BU16 += 8;             // 16-bit rows: BU16 / 2 words
+        // 16-bit rows: the same choice over pitches = 0..56 (mod 64) halves
+        const int base16 = (std::max(need, 8) + 7) / 8 * 8;
+        int BU16 = base16;
+        while (BU16 % 16 != 8) BU16 += 8;
+        best = -1.0;
+        for (int r = 0; r < 64; r += 8) {
+            int bu = base16;
+            while (bu % 64 != r) bu += 8;
+            if (bu > 256 || 2.0 * bu * BV * 2 > 96.0 * 1024) continue;
+            const double c = bp_bank_cost(plan, bu, 2, bx, bz);
+            if (best < 0.0 || c < best || (c == best && bu < BU16)) { best = c; BU16 = bu; }
+        }
         if (const char* ov = std::getenv("TIGRE_B200_BP_BOX")) {   // test hook: force a box (e.g. "8x4")
             int bu = 0, bv = 0;
             if (std::sscanf(ov, "%dx%d", &bu, &bv) == 2 && bu > 0 && bv > 0) {
@@ -541,7 +552,7 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
                 BV = bv;
             }
         }
-        const bool ok = std::isfinite(ext_u) && std::isfinite(ext_v) && BU16 <= 256 && BV <= 256 &&
+        const bool ok = std::isfinite(ext_u) && std::isfinite(ext_v) && BU <= 256 && BU16 <= 256 && BV <= 256 &&
                         2.0 * BU * BV * 4 <= 96.0 * 1024 && std::getenv("TIGRE_B200_NO_TMA") == nullptr;
         plan->bp_box_u = ok ? BU : 0;
         plan->bp_box_u16 = ok ? BU16 : 0;
