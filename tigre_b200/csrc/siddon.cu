@@ -23,6 +23,8 @@
 
 #include <cmath>
 
+#include <cstdlib>
+
 #include "tigre_internal.h"
 
 namespace tigre {
@@ -40,6 +42,7 @@ struct SiddonArgs {
     int zpad;                    // zero slices before and after each z-run of the z-fast copy
     int parallel;                // parallel beam: each pixel's source is s + u du + v dv
     int* status;                 // plan status word (bit 1: a ray outside the host's z bound)
+    int grid_nug, grid_nviews, grid_vtile;   // cell kernel: 1-D grid of u groups x views x row bands
 };
 
 constexpr float kInf = __builtin_huge_valf();
@@ -392,11 +395,22 @@ __global__ void __launch_bounds__(128, R >= 8 ? 4 : 6) siddon_cells_kernel(Siddo
     static_assert(R % 2 == 0, "rows are processed in pairs");
     constexpr int H = R / 2;
     const int lane = threadIdx.x & 31;
-    const int u = blockIdx.x * 4 + (threadIdx.x >> 5);
-    const int la = blockIdx.y;
+    // Block order: row band slowest, then tiles of grid_vtile views; inside a tile the views
+    // vary fastest, so the blocks resident at one time are a few u groups of many
+    // neighbouring views, whose rays cross nearly the same voxel columns (L2 reuse).
+    const long per_band = (long)p.grid_nug * p.grid_nviews;
+    const int band = (int)(blockIdx.x / per_band);
+    const long rr = blockIdx.x - (long)band * per_band;
+    const long tile_blocks = (long)p.grid_nug * p.grid_vtile;
+    const int vt = (int)(rr / tile_blocks);
+    const int r2 = (int)(rr - (long)vt * tile_blocks);
+    const int tsize = min(p.grid_vtile, p.grid_nviews - vt * p.grid_vtile);
+    const int ug = r2 / tsize;
+    const int la = vt * p.grid_vtile + (r2 - ug * tsize);
+    const int u = ug * 4 + (threadIdx.x >> 5);
     if (u >= p.nU) return;
     const FrameSiddon& F = p.frames[p.a0 + la];
-    const int vbase = blockIdx.z * (32 * R) + lane;
+    const int vbase = band * (32 * R) + lane;
     TP* out = (TP*)p.proj + (size_t)la * p.nV * p.nU + u;
     // ---- shared xy ray ----
     const double sx = p.parallel ? fma((double)u, F.du[0], F.s[0]) : F.s[0];
@@ -650,12 +664,22 @@ int launch_siddon_cells(TigrePlan* P, const void* vol_z, int vdt, void* proj, in
     const int nv = P->d.nV;
     // rows per thread: 8 (256 rows per warp, 4 resident blocks per SM) for tall detectors
     const int R = nv >= 512 ? 8 : (nv >= 256 ? 4 : 2);
+    static const int vtile_env = [] {
+        const char* e = std::getenv("TIGRE_B200_SIDDON_VIEW_TILE");   // tuning hook
+        return e ? std::max(1, std::atoi(e)) : 0;
+    }();
+    const int vtile = vtile_env ? vtile_env : 64;   // flat between 32 and 128 views at 512^3 / 1024x768
     const int na = a1 - a0;
-    for (int c = 0; c < na; c += 65535) {
+    const int nug = (P->d.nU + 3) / 4, nbands = (nv + 32 * R - 1) / (32 * R);
+    const long max_views = std::max(1L, (long)INT32_MAX / ((long)nug * nbands));
+    for (long c = 0; c < na; c += max_views) {
         SiddonArgs ac = a;
-        ac.a0 = a0 + c;
+        ac.a0 = a0 + (int)c;
         ac.proj = (char*)proj + (size_t)c * P->d.nU * P->d.nV * dtype_size(pdt);
-        dim3 grid((P->d.nU + 3) / 4, std::min(65535, na - c), (nv + 32 * R - 1) / (32 * R));
+        ac.grid_nug = nug;
+        ac.grid_nviews = (int)std::min<long>(max_views, na - c);
+        ac.grid_vtile = std::min(vtile, ac.grid_nviews);
+        dim3 grid((unsigned)((long)nug * ac.grid_nviews * nbands));
         if (vdt == TIGRE_F32 && pdt == TIGRE_F32) launch_cells_typed<float, float>(ac, R, grid, st);
         else if (vdt == TIGRE_BF16 && pdt == TIGRE_BF16) launch_cells_typed<__nv_bfloat16, __nv_bfloat16>(ac, R, grid, st);
         else if (vdt == TIGRE_F16 && pdt == TIGRE_F16) launch_cells_typed<__half, __half>(ac, R, grid, st);
