@@ -281,7 +281,8 @@ def main():
     atb_launch = t_atb / args.steps
     if ax_launch >= atb_launch:
         alg = nseg * 4 + rays * 4           # one voxel gather per Siddon segment + one output write per ray
-        roof = {"kernel": "siddon_cells_kernel<float,float,4>", "bound": "hbm",
+        rpt = 8 if NV >= 512 else (4 if NV >= 256 else 2)   # rows per thread, as the launcher picks
+        roof = {"kernel": "siddon_cells_kernel<float,float,%d>" % rpt, "bound": "hbm",
                 "achieved": alg / ax_launch / 1e9, "alg_bytes_per_launch": alg,
                 "traffic": _scaled_traffic("siddon", NA)}
     else:
@@ -331,17 +332,18 @@ def main():
         dist.destroy_process_group()
 
 
-# DRAM bytes per view of the Siddon launch on the 512^3 workload, from an ncu capture of 36 views
-# (dram__bytes_read.sum + dram__bytes_write.sum = 10.337 GB; profiles/siddon_cells_512cube_36views.txt),
-# scaled to the timed launch by its view count: each view re-reads the part of the volume it crosses
-# and writes its projection once.  The backprojector's DRAM traffic is one volume write plus one
-# read of the projections, not proportional to the views, so it is not scaled.
-TRAFFIC_PER_VIEW = {"siddon": 287152417, "bp": None}
+# DRAM bytes of one launch on the 512^3 / 1024x768 / 720-view workload, from a single-pass ncu
+# capture of that launch (dram__bytes_read.sum + dram__bytes_write.sum;
+# profiles/launches_512cube_720views.txt gives the command).  Neither kernel's traffic is
+# proportional to the view count (the Siddon grid reuses voxel columns across a tile of 64 views
+# in L2; the backprojector reads each view's patches once per voxel block), so the figure is
+# reported only for that exact launch.
+TRAFFIC_720_VIEWS = {"siddon": 6644203008 + 2288307968, "bp": 17286047744 + 527202816}
 
 
 def _scaled_traffic(kind, views):
-    per_view = TRAFFIC_PER_VIEW.get(kind) if NVOX == (512, 512, 512) and NU == 1024 else None
-    return None if per_view is None else int(per_view * views)
+    exact = NVOX == (512, 512, 512) and NU == 1024 and NV == 768 and views == 720
+    return TRAFFIC_720_VIEWS.get(kind) if exact else None
 
 
 def time_ops(P, plan, vol, proj, reps=3):

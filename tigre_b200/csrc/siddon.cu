@@ -379,6 +379,7 @@ __global__ void __launch_bounds__(128, 6) siddon_columns_kernel(SiddonArgs p) {
 // its float bits index the column directly.  The pads (at least the largest z extent of
 // any ray inside the xy box, from the host) make every index valid without clamping:
 // a ray whose z range misses the volume reads one zero slice.
+constexpr int kCellWarps = 4;                  // warps (neighbouring detector columns) per block
 constexpr float kMagic = 12582912.0f;          // 1.5 * 2^23
 constexpr unsigned kMagicBits = 0x4B400000u;   // its bit pattern
 
@@ -391,7 +392,7 @@ __device__ __forceinline__ float ldz(uintptr_t cb, float t) {
 }
 
 template <typename TV, typename TP, int R>
-__global__ void __launch_bounds__(128, R >= 8 ? 4 : 6) siddon_cells_kernel(SiddonArgs p) {
+__global__ void __launch_bounds__(32 * kCellWarps, (R >= 8 ? 16 : 24) / kCellWarps) siddon_cells_kernel(SiddonArgs p) {
     static_assert(R % 2 == 0, "rows are processed in pairs");
     constexpr int H = R / 2;
     const int lane = threadIdx.x & 31;
@@ -407,7 +408,7 @@ __global__ void __launch_bounds__(128, R >= 8 ? 4 : 6) siddon_cells_kernel(Siddo
     const int tsize = min(p.grid_vtile, p.grid_nviews - vt * p.grid_vtile);
     const int ug = r2 / tsize;
     const int la = vt * p.grid_vtile + (r2 - ug * tsize);
-    const int u = ug * 4 + (threadIdx.x >> 5);
+    const int u = ug * kCellWarps + (threadIdx.x >> 5);
     if (u >= p.nU) return;
     const FrameSiddon& F = p.frames[p.a0 + la];
     const int vbase = band * (32 * R) + lane;
@@ -650,9 +651,9 @@ int launch_siddon_columns(TigrePlan* P, const void* vol_z, int vdt, void* proj, 
 
 template <typename TV, typename TP>
 static void launch_cells_typed(const SiddonArgs& a, int rows_per_thread, dim3 grid, cudaStream_t st) {
-    if (rows_per_thread == 8) siddon_cells_kernel<TV, TP, 8><<<grid, 128, 0, st>>>(a);
-    else if (rows_per_thread == 4) siddon_cells_kernel<TV, TP, 4><<<grid, 128, 0, st>>>(a);
-    else siddon_cells_kernel<TV, TP, 2><<<grid, 128, 0, st>>>(a);
+    if (rows_per_thread == 8) siddon_cells_kernel<TV, TP, 8><<<grid, 32 * kCellWarps, 0, st>>>(a);
+    else if (rows_per_thread == 4) siddon_cells_kernel<TV, TP, 4><<<grid, 32 * kCellWarps, 0, st>>>(a);
+    else siddon_cells_kernel<TV, TP, 2><<<grid, 32 * kCellWarps, 0, st>>>(a);
 }
 
 int launch_siddon_cells(TigrePlan* P, const void* vol_z, int vdt, void* proj, int pdt, int a0, int a1,
@@ -670,7 +671,7 @@ int launch_siddon_cells(TigrePlan* P, const void* vol_z, int vdt, void* proj, in
     }();
     const int vtile = vtile_env ? vtile_env : 64;   // flat between 32 and 128 views at 512^3 / 1024x768
     const int na = a1 - a0;
-    const int nug = (P->d.nU + 3) / 4, nbands = (nv + 32 * R - 1) / (32 * R);
+    const int nug = (P->d.nU + kCellWarps - 1) / kCellWarps, nbands = (nv + 32 * R - 1) / (32 * R);
     const long max_views = std::max(1L, (long)INT32_MAX / ((long)nug * nbands));
     for (long c = 0; c < na; c += max_views) {
         SiddonArgs ac = a;
