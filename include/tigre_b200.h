@@ -117,6 +117,20 @@ int tigre_voxel_backprojection2(const float* projections, const TigreGeometry* g
 int tigre_pocs_tv(const float* img, float* dst, float alpha, const long* image_size, int max_iter,
                   const int* gpu_ids, int n_gpus);
 
+/* Adaptive-weighted TV descent: as tigre_pocs_tv with each difference component weighted by
+ * exp(-(d/delta)^2).  Replaces aw_pocs_tv (Common/CUDA/GD_AwTV.hpp:58, GD_AwTV.cu:276), the
+ * operator behind tigre.utilities.AwminTV (_AwminTV.pyx). */
+int tigre_aw_pocs_tv(const float* img, float* dst, float alpha, const long* image_size, int max_iter, float delta,
+                     const int* gpu_ids, int n_gpus);
+
+/* PICCS TV descent: maxIter steps of img -= alpha*g/|g| with
+ * g = (1-ratio) grad TV(img) + ratio grad TV(img - prior), one-sided differences at every face.
+ * Replaces piccs_tv (Common/CUDA/PICCS.hpp:58, PICCS.cu:274), behind
+ * tigre.utilities.minPICCS (_minPICCS.pyx).  As the reference, |g| has no epsilon: a
+ * constant image and prior give NaN. */
+int tigre_piccs_tv(const float* img, const float* prior, float* dst, float alpha, float ratio, const long* image_size,
+                   int max_iter, const int* gpu_ids, int n_gpus);
+
 /* TV denoising by the primal-dual iteration of tvdenoising (Common/CUDA/tv_proximal.hpp,
  * tv_proximal.cu:185), the operator behind tigre.utilities.im3ddenoise (_tv_proximal.pyx).
  * src, dst: (nZ, nY, nX) float32 host arrays; image_size = {nX, nY, nZ}; spacing = {dX, dY, dZ}. */
@@ -195,6 +209,12 @@ int tigre_tv_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha
  * address with that device current; make it before any stream capture. */
 int tigre_tv_pocs_noalloc(void* d_img, int dtype, long nx, long ny, long nz, float alpha, int max_iter,
                           float* d_work, void* stream);
+/* Device counterparts of tigre_aw_pocs_tv and tigre_piccs_tv, in place on d_img; d_work:
+ * nx*ny*nz floats of caller scratch; d_prior: the prior image (FP32, same layout). */
+int tigre_tv_aw_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha, int max_iter, float delta,
+                     float* d_work, void* stream);
+int tigre_tv_piccs(void* d_img, const void* d_prior, int dtype, long nx, long ny, long nz, float alpha, float ratio,
+                   int max_iter, float* d_work, void* stream);
 /* Device TV denoising (same iteration as tigre_tvdenoising) of d_src into d_dst (may alias);
  * d_work: tigre_tv_denoise_work_floats(nx, ny, nz) floats of caller scratch. */
 long long tigre_tv_denoise_work_floats(long nx, long ny, long nz);

@@ -7,6 +7,9 @@
 //   Common/CUDA/voxel_backprojection.hpp:52       voxel_backprojection
 //   Common/CUDA/voxel_backprojection2.hpp:57      voxel_backprojection2
 //   Common/CUDA/GD_TV.hpp:58                      pocs_tv
+//   Common/CUDA/GD_AwTV.hpp:58                    aw_pocs_tv
+//   Common/CUDA/PICCS.hpp:58                      piccs_tv
+//   Common/CUDA/tv_proximal.hpp:52                tvdenoising
 //   and the *_parallel symbols referenced by _Ax.pyx:21-26 / _Atb.pyx:21-22.
 //
 // `Geometry` and `GpuIds` here are declared with the field layout of
@@ -65,6 +68,11 @@ int voxel_backprojection_parallel(float* projections, Geometry geo, float* resul
                                   int nalpha, const GpuIds& gpuids);
 // The reference returns void here; errors are reported on stderr and leave dst unchanged.
 void pocs_tv(float* img, float* dst, float alpha, const long* image_size, int maxIter, const GpuIds& gpuids);
+// Common/CUDA/GD_AwTV.hpp:58 and PICCS.hpp:58; void like the reference, errors on stderr.
+void aw_pocs_tv(float* img, float* dst, float alpha, const long* image_size, int maxIter, const float delta,
+                const GpuIds& gpuids);
+void piccs_tv(const float* img, const float* prior, float* dst, float alpha, float ratio, const long* image_size,
+              int maxIter, const GpuIds& gpuids);
 // Common/CUDA/tv_proximal.hpp:52: TV denoising (im3ddenoise); void like the reference, errors on stderr.
 void tvdenoising(float* src, float* dst, float lambda, const float* spacing, const long* image_size, int maxIter,
                 const GpuIds& gpuids);

@@ -34,6 +34,9 @@ REF_GROUPS = {
     "tv": (["TIGRE_common.cpp", "GpuIds.cpp", "gpuUtils.cu", "GD_TV.cu"], "REF_TV"),
     # a separate extension in the reference too (_tv_proximal): it repeats helpers of GD_TV.cu
     "prox": (["TIGRE_common.cpp", "GpuIds.cpp", "gpuUtils.cu", "tv_proximal.cu"], "REF_PROX"),
+    # _AwminTV and _minPICCS are separate extensions too (each repeats GD_TV.cu's helpers)
+    "awtv": (["TIGRE_common.cpp", "GpuIds.cpp", "gpuUtils.cu", "GD_AwTV.cu"], "REF_AWTV"),
+    "piccs": (["TIGRE_common.cpp", "GpuIds.cpp", "gpuUtils.cu", "PICCS.cu"], "REF_PICCS"),
 }
 
 

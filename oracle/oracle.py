@@ -62,6 +62,10 @@ def lib():
                                                      C.c_int]
         _LIB.oracle_tv_gradient.argtypes = [f, C.c_long, C.c_long, C.c_long, f, C.c_int]
         _LIB.oracle_pocs_tv.argtypes = [f, f, C.c_float, C.c_long, C.c_long, C.c_long, C.c_int, C.c_int]
+        _LIB.oracle_aw_pocs_tv.argtypes = [f, f, C.c_float, C.c_float, C.c_long, C.c_long, C.c_long, C.c_int,
+                                           C.c_int]
+        _LIB.oracle_piccs_tv.argtypes = [f, f, f, C.c_float, C.c_float, C.c_long, C.c_long, C.c_long, C.c_int,
+                                         C.c_int]
     return _LIB
 
 
@@ -170,6 +174,28 @@ def pocs_tv(img, alpha, maxiter, nthreads=0):
     out = np.empty_like(img)
     lib().oracle_pocs_tv(img.ctypes.data, out.ctypes.data, float(alpha), nx, ny, nz, int(maxiter),
                          _threads(nthreads))
+    return out
+
+
+def aw_pocs_tv(img, alpha, maxiter, delta, nthreads=0):
+    """aw_pocs_tv (Common/CUDA/GD_AwTV.cu:276-720) in FP64."""
+    img = _f32(img)
+    nz, ny, nx = img.shape
+    out = np.empty_like(img)
+    lib().oracle_aw_pocs_tv(img.ctypes.data, out.ctypes.data, float(alpha), float(delta), nx, ny, nz, int(maxiter),
+                            _threads(nthreads))
+    return out
+
+
+def piccs_tv(img, prior, alpha, ratio, maxiter, nthreads=0):
+    """piccs_tv (Common/CUDA/PICCS.cu:274-380) in FP64."""
+    img, prior = _f32(img), _f32(prior)
+    if prior.shape != img.shape:
+        raise ValueError("prior and image sizes differ")
+    nz, ny, nx = img.shape
+    out = np.empty_like(img)
+    lib().oracle_piccs_tv(img.ctypes.data, prior.ctypes.data, out.ctypes.data, float(alpha), float(ratio), nx, ny, nz,
+                          int(maxiter), _threads(nthreads))
     return out
 
 

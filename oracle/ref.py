@@ -45,7 +45,7 @@ class Geometry(C.Structure):
 
 
 def available() -> bool:
-    return all(os.path.exists(os.path.join(REF_DIR, "libref_%s.so" % g)) for g in ("ax", "atb", "tv", "prox"))
+    return all(os.path.exists(os.path.join(REF_DIR, "libref_%s.so" % g)) for g in ("ax", "atb", "tv", "prox", "awtv", "piccs"))
 
 
 def _geo_dict(geo, angles):
@@ -145,6 +145,28 @@ def _worker(spec_path):
             L.ref_tvdenoise(inp.ctypes.data, out.ctypes.data, float(spec["lmbda"]), C.cast(size, C.c_void_p),
                             int(spec["maxiter"]), dev)
             times.append(time.perf_counter() - t)
+    elif op == "aw_pocs_tv":
+        L = C.CDLL(os.path.join(REF_DIR, "libref_awtv.so"))
+        L.ref_aw_pocs_tv.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_int, C.c_float, C.c_int]
+        out = np.empty_like(inp)
+        size = (C.c_long * 3)(inp.shape[2], inp.shape[1], inp.shape[0])
+        for _ in range(int(spec.get("repeat", 1))):
+            t = time.perf_counter()
+            L.ref_aw_pocs_tv(inp.ctypes.data, out.ctypes.data, float(spec["alpha"]), C.cast(size, C.c_void_p),
+                             int(spec["maxiter"]), float(spec["delta"]), dev)
+            times.append(time.perf_counter() - t)
+    elif op == "piccs_tv":
+        L = C.CDLL(os.path.join(REF_DIR, "libref_piccs.so"))
+        L.ref_piccs_tv.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_int,
+                                   C.c_int]
+        prior = np.ascontiguousarray(np.load(spec["prior"]), dtype=np.float32)
+        out = np.empty_like(inp)
+        size = (C.c_long * 3)(inp.shape[2], inp.shape[1], inp.shape[0])
+        for _ in range(int(spec.get("repeat", 1))):
+            t = time.perf_counter()
+            L.ref_piccs_tv(inp.ctypes.data, prior.ctypes.data, out.ctypes.data, float(spec["alpha"]),
+                           float(spec["ratio"]), C.cast(size, C.c_void_p), int(spec["maxiter"]), dev)
+            times.append(time.perf_counter() - t)
     else:
         raise SystemExit("unknown op " + op)
     np.save(spec["output"], out)
@@ -161,6 +183,10 @@ def _run(op, inp, geo=None, angles=None, repeat=1, device=0, timeout=1800, **ext
         if geo is not None:
             spec["geo"] = _geo_dict(geo, angles)
         np.save(spec["input"], np.ascontiguousarray(inp, dtype=np.float32))
+        if "prior_array" in extra:
+            spec.pop("prior_array")
+            spec["prior"] = os.path.join(td, "prior.npy")
+            np.save(spec["prior"], np.ascontiguousarray(extra["prior_array"], dtype=np.float32))
         sp = os.path.join(td, "spec.json")
         json.dump(spec, open(sp, "w"))
         r = subprocess.run([sys.executable, os.path.abspath(__file__), "--worker", sp], capture_output=True,
@@ -187,13 +213,26 @@ def pocs_tv(img, alpha, maxiter, repeat=1, device=0):
     return _run("pocs_tv", img, alpha=float(alpha), maxiter=int(maxiter), repeat=repeat, device=device)
 
 
+
+def tvdenoise(img, lmbda, maxiter, repeat=1, device=0):
+    """The reference's tvdenoising on img (already scaled as im3ddenoise scales it)."""
+    return _run("tvdenoise", img, lmbda=float(lmbda), maxiter=int(maxiter), repeat=repeat, device=device)
+
+
+def aw_pocs_tv(img, alpha, maxiter, delta, repeat=1, device=0):
+    """The reference's aw_pocs_tv (AwminTV)."""
+    return _run("aw_pocs_tv", img, alpha=float(alpha), maxiter=int(maxiter), delta=float(delta), repeat=repeat,
+                device=device)
+
+
+def piccs_tv(img, prior, alpha, ratio, maxiter, repeat=1, device=0):
+    """The reference's piccs_tv (minPICCS)."""
+    return _run("piccs_tv", img, alpha=float(alpha), ratio=float(ratio), maxiter=int(maxiter), repeat=repeat,
+                device=device, prior_array=prior)
+
+
 if __name__ == "__main__":
     if len(sys.argv) == 3 and sys.argv[1] == "--worker":
         _worker(sys.argv[2])
     else:
         print(__doc__)
-
-
-def tvdenoise(img, lmbda, maxiter, repeat=1, device=0):
-    """The reference's tvdenoising on img (already scaled as im3ddenoise scales it)."""
-    return _run("tvdenoise", img, lmbda=float(lmbda), maxiter=int(maxiter), repeat=repeat, device=device)

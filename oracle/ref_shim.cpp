@@ -26,6 +26,10 @@
 #include "GD_TV.hpp"
 #elif defined(REF_PROX)
 #include "tv_proximal.hpp"
+#elif defined(REF_AWTV)
+#include "GD_AwTV.hpp"
+#elif defined(REF_PICCS)
+#include "PICCS.hpp"
 #endif
 
 namespace {
@@ -83,6 +87,21 @@ int ref_tvdenoise(float* img, float* dst, float lambda, const long* image_size, 
     OneGpu g(dev);
     const float spacing[3] = {1.f, 1.f, 1.f};
     tvdenoising(img, dst, lambda, spacing, image_size, maxiter, g.ids);
+    return 0;
+}
+#elif defined(REF_AWTV)
+// aw_pocs_tv (GD_AwTV.cu:276); image_size = {nX, nY, nZ}.
+int ref_aw_pocs_tv(float* img, float* dst, float alpha, const long* image_size, int maxiter, float delta, int dev) {
+    OneGpu g(dev);
+    aw_pocs_tv(img, dst, alpha, image_size, maxiter, delta, g.ids);
+    return 0;
+}
+#elif defined(REF_PICCS)
+// piccs_tv (PICCS.cu:274); image_size = {nX, nY, nZ}; ends with cudaDeviceReset().
+int ref_piccs_tv(float* img, float* prior, float* dst, float alpha, float ratio, const long* image_size, int maxiter,
+                 int dev) {
+    OneGpu g(dev);
+    piccs_tv(img, prior, dst, alpha, ratio, image_size, maxiter, g.ids);
     return 0;
 }
 #endif

@@ -4,7 +4,7 @@
 
 Each fixture stores the case name, the seed and the reference's outputs for
 Siddon and interpolated projection, FDK and matched backprojection (of the
-reference's own Siddon projections) and pocs_tv.  Inputs are regenerated
+reference's own Siddon projections), pocs_tv, tvdenoising, aw_pocs_tv and piccs_tv.  Inputs are regenerated
 from the seed by tests/geometries.py, so only outputs are stored.
 """
 import os
@@ -20,12 +20,25 @@ from tests import golden_cases as GC  # noqa: E402
 
 
 def main():
-    # usage: make_golden.py [OUT_DIR [CASE ...]]   (default: this directory, every case)
-    out_dir = sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__))
-    names = sys.argv[2:] or GC.CASES
+    # usage: make_golden.py [--keys k1,k2] [OUT_DIR [CASE ...]]   (default: this directory, every case)
+    # --keys computes only those outputs and merges them into the fixtures already in OUT_DIR.
+    args = sys.argv[1:]
+    keys = None
+    if args[:1] == ["--keys"]:
+        keys = set(args[1].split(","))
+        args = args[2:]
+    out_dir = args[0] if args else os.path.dirname(os.path.abspath(__file__))
+    names = args[1:] or GC.CASES
     os.makedirs(out_dir, exist_ok=True)
     for name in names:
         geo, ang, img = GC.make(name)
+        path = os.path.join(out_dir, "ref_%s.npz" % name)
+        if keys is not None:
+            res = dict(np.load(path))
+            _tv_family(res, img, keys)
+            np.savez_compressed(path, **res)
+            print(name, "updated", sorted(keys))
+            continue
         res = {}
         res["siddon"], _ = ref.ax(img, geo, ang, "Siddon")
         res["interpolated"], _ = ref.ax(img, geo, ang, "interpolated")
@@ -34,8 +47,17 @@ def main():
         res["pocs_tv"], _ = ref.pocs_tv(img, GC.TV_ALPHA, GC.TV_ITERS)
         scaled = (img - img.min()) / (img - img.min()).max()
         res["tvdenoise"], _ = ref.tvdenoise(scaled.astype(np.float32), GC.DENOISE_LAMBDA, GC.DENOISE_ITERS)
-        np.savez_compressed(os.path.join(out_dir, "ref_%s.npz" % name), **res)
+        _tv_family(res, img, {"awtv", "piccs"})
+        np.savez_compressed(path, **res)
         print(name, {k: v.shape for k, v in res.items()})
+
+
+def _tv_family(res, img, keys):
+    """AwminTV and minPICCS outputs of the reference (aw_pocs_tv, piccs_tv)."""
+    if "awtv" in keys:
+        res["awtv"], _ = ref.aw_pocs_tv(img, GC.TV_ALPHA, GC.TV_ITERS, GC.AWTV_DELTA)
+    if "piccs" in keys:
+        res["piccs"], _ = ref.piccs_tv(img, GC.piccs_prior(img), GC.TV_ALPHA, GC.PICCS_RATIO, GC.TV_ITERS)
 
 
 if __name__ == "__main__":

@@ -8,6 +8,14 @@ TV_ALPHA = 0.002
 TV_ITERS = 10
 DENOISE_LAMBDA = 15.0
 DENOISE_ITERS = 30
+AWTV_DELTA = -0.005       # AwminTV's default delta (_AwminTV.pyx:33)
+PICCS_RATIO = 0.95        # minPICCS's default ratio (_minPICCS.pyx:39)
+
+
+def piccs_prior(img):
+    """Prior image of the PICCS fixtures: the image shifted by one voxel in x and y, scaled by 0.9."""
+    return (0.9 * np.roll(np.roll(img, 1, axis=2), 1, axis=1)).astype(np.float32)
+
 
 CASES = ("small", "offsets", "parallel")
 

@@ -121,6 +121,44 @@ def test_tv_gradient_and_pocs_match_oracle():
     assert mx <= TOL and l2 <= TOL, (mx, l2)
 
 
+@pytest.mark.parametrize("shape", [(24, 31, 29), (1, 17, 13), (2, 9, 40)])
+def test_awtv_matches_oracle(shape):
+    """AwminTV (aw_pocs_tv, GD_AwTV.cu:276): host entry point and device path against the
+    oracle, at the default delta and at one of the order of the differences."""
+    torch = _torch()
+    import tigre_b200 as tigre
+    rng = np.random.default_rng(21)
+    img = (G.phantom(shape, seed=21) + rng.normal(0, 1e-3, shape)).astype(np.float32)
+    for delta in (-0.005, 0.02):
+        ref = O.aw_pocs_tv(img, 0.002, 15, delta)
+        out = tigre.AwminTV(img, alpha=0.002, maxiter=15, delta=delta)
+        mx, l2 = G.rel_err(out, ref)
+        assert mx <= TOL and l2 <= TOL, ("host", delta, mx, l2)
+        dev = tigre.AwminTV(torch.from_numpy(img).cuda(), alpha=0.002, maxiter=15, delta=delta).cpu().numpy()
+        mx, l2 = G.rel_err(dev, ref)
+        assert mx <= TOL and l2 <= TOL, ("device", delta, mx, l2)
+
+
+@pytest.mark.parametrize("shape", [(24, 31, 29), (1, 17, 13), (3, 8, 33)])
+def test_piccs_matches_oracle(shape):
+    """minPICCS (piccs_tv, PICCS.cu:274): host entry point and device path against the oracle."""
+    torch = _torch()
+    import tigre_b200 as tigre
+    from tests import golden_cases as GC
+    rng = np.random.default_rng(22)
+    img = (G.phantom(shape, seed=22) + rng.normal(0, 1e-3, shape)).astype(np.float32)
+    prior = GC.piccs_prior(img)
+    for ratio in (0.95, 0.5):
+        ref = O.piccs_tv(img, prior, 0.002, ratio, 15)
+        out = tigre.minPICCS(img, prior, alpha=0.002, maxiter=15, ratio=ratio)
+        mx, l2 = G.rel_err(out, ref)
+        assert mx <= TOL and l2 <= TOL, ("host", ratio, mx, l2)
+        dev = tigre.minPICCS(torch.from_numpy(img).cuda(), torch.from_numpy(prior).cuda(), alpha=0.002, maxiter=15,
+                             ratio=ratio).cpu().numpy()
+        mx, l2 = G.rel_err(dev, ref)
+        assert mx <= TOL and l2 <= TOL, ("device", ratio, mx, l2)
+
+
 def test_tv_value_consistent_with_gradient():
     """Central differences of tv_value reproduce tv_gradient (noisy volume, |grad| >> eps)."""
     torch = _torch()

@@ -16,6 +16,8 @@ from .utilities.geometry import ConeGeometryDefault as geometry_default  # noqa:
 from .utilities.Ax import Ax  # noqa: F401
 from .utilities.Atb import Atb  # noqa: F401
 from .utilities.minTV import minTV  # noqa: F401
+from .utilities.AwminTV import AwminTV  # noqa: F401
+from .utilities.minPICCS import minPICCS  # noqa: F401
 from .utilities.gpu import GpuIds, getGpuIds, getGpuNames  # noqa: F401
 
 __version__ = "1.0.0"

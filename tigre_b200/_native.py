@@ -91,6 +91,14 @@ _SIGS = {
                                         C.c_void_p, C.c_void_p]),
     "tigre_tvdenoising": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                     C.c_int]),
+    "tigre_aw_pocs_tv": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_int, C.c_float, C.c_void_p,
+                                   C.c_int]),
+    "tigre_piccs_tv": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_int,
+                                 C.c_void_p, C.c_int]),
+    "tigre_tv_aw_pocs": (C.c_int, [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_int, C.c_float,
+                                   C.c_void_p, C.c_void_p]),
+    "tigre_tv_piccs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_float,
+                                 C.c_int, C.c_void_p, C.c_void_p]),
     "tigre_tv_denoise_work_floats": (C.c_longlong, [C.c_long, C.c_long, C.c_long]),
     "tigre_tv_denoise": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long, C.c_long, C.c_long, C.c_float, C.c_void_p,
                                    C.c_int, C.c_void_p, C.c_void_p]),

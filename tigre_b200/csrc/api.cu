@@ -376,6 +376,35 @@ int host_pocs_tv(const float* img, float* dst, float alpha, const long* image_si
     return TIGRE_SUCCESS;
 }
 
+int host_weighted_tv(int kind, const float* img, const float* prior, float* dst, float alpha, float param,
+                     const long* image_size, int max_iter, const int* ids, int n) {
+    if (!img || !dst || !image_size || (kind == 1 && !prior)) return fail(TIGRE_ERR_BAD_ASSERT, "null argument");
+    const long nx = image_size[0], ny = image_size[1], nz = image_size[2];
+    if (nx <= 0 || ny <= 0 || nz <= 0) return fail(TIGRE_ERR_BAD_ASSERT, "bad image size");
+    int dev = 0;
+    if (int rc = pick_device(ids, n, &dev)) return rc;
+    DeviceGuard g(dev);
+    DeviceState* S = state(dev);
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (int rc = S->init(dev)) return rc;
+    const size_t nvox = (size_t)nx * ny * nz;
+    void *dimg = nullptr, *dwork = nullptr, *dprior = nullptr;
+    if (int rc = S->get(0, nvox * sizeof(float), &dimg)) return rc;
+    if (int rc = S->get(1, nvox * sizeof(float), &dwork)) return rc;
+    TIGRE_CUDA(cudaMemcpyAsync(dimg, img, nvox * sizeof(float), cudaMemcpyHostToDevice, S->st));
+    if (kind == 1) {
+        if (int rc = S->get(2, nvox * sizeof(float), &dprior)) return rc;
+        TIGRE_CUDA(cudaMemcpyAsync(dprior, prior, nvox * sizeof(float), cudaMemcpyHostToDevice, S->st));
+        if (int rc = tigre_tv_piccs(dimg, dprior, TIGRE_F32, nx, ny, nz, alpha, param, max_iter, (float*)dwork, S->st))
+            return rc;
+    } else if (int rc = tigre_tv_aw_pocs(dimg, TIGRE_F32, nx, ny, nz, alpha, max_iter, param, (float*)dwork, S->st)) {
+        return rc;
+    }
+    TIGRE_CUDA(cudaMemcpyAsync(dst, dimg, nvox * sizeof(float), cudaMemcpyDeviceToHost, S->st));
+    TIGRE_CUDA(cudaStreamSynchronize(S->st));
+    return TIGRE_SUCCESS;
+}
+
 int host_tvdenoising(const float* src, float* dst, float lambda, const float* spacing, const long* image_size,
                      int max_iter, const int* ids, int n) {
     if (!src || !dst || !image_size) return fail(TIGRE_ERR_BAD_ASSERT, "null argument");
@@ -437,6 +466,16 @@ int tigre_voxel_backprojection2(const float* proj, const TigreGeometry* geo, flo
 int tigre_pocs_tv(const float* img, float* dst, float alpha, const long* image_size, int max_iter, const int* ids,
                   int n) {
     return host_pocs_tv(img, dst, alpha, image_size, max_iter, ids, n);
+}
+
+int tigre_aw_pocs_tv(const float* img, float* dst, float alpha, const long* image_size, int max_iter, float delta,
+                     const int* ids, int n) {
+    return host_weighted_tv(0, img, nullptr, dst, alpha, delta, image_size, max_iter, ids, n);
+}
+
+int tigre_piccs_tv(const float* img, const float* prior, float* dst, float alpha, float ratio, const long* image_size,
+                   int max_iter, const int* ids, int n) {
+    return host_weighted_tv(1, img, prior, dst, alpha, ratio, image_size, max_iter, ids, n);
 }
 
 int tigre_tvdenoising(const float* src, float* dst, float lambda, const float* spacing, const long* image_size,

@@ -56,6 +56,19 @@ void pocs_tv(float* img, float* dst, float alpha, const long* image_size, int ma
     if (rc) std::fprintf(stderr, "minimizeTV:POCS_TV: error %d: %s\n", rc, tigre_last_error());
 }
 
+void aw_pocs_tv(float* img, float* dst, float alpha, const long* image_size, int maxIter, const float delta,
+                const GpuIds& ids) {
+    const int rc = tigre_aw_pocs_tv(img, dst, alpha, image_size, maxIter, delta, ids.m_piDeviceIds, ids.m_iCount);
+    if (rc) std::fprintf(stderr, "minimizeAwTV:GD_AwTV: error %d: %s\n", rc, tigre_last_error());
+}
+
+void piccs_tv(const float* img, const float* prior, float* dst, float alpha, float ratio, const long* image_size,
+              int maxIter, const GpuIds& ids) {
+    const int rc =
+        tigre_piccs_tv(img, prior, dst, alpha, ratio, image_size, maxIter, ids.m_piDeviceIds, ids.m_iCount);
+    if (rc) std::fprintf(stderr, "minimizeTV:PICCS_TV: error %d: %s\n", rc, tigre_last_error());
+}
+
 void tvdenoising(float* src, float* dst, float lambda, const float* spacing, const long* image_size, int maxIter,
                  const GpuIds& ids) {
     const int rc = tigre_tvdenoising(src, dst, lambda, spacing, image_size, maxIter, ids.m_piDeviceIds, ids.m_iCount);

@@ -149,6 +149,117 @@ __global__ void __launch_bounds__(256) tv_value_kernel(const float* __restrict__
     if (threadIdx.x == 0) atomicAdd(out, s);
 }
 
+// ---- adaptive-weighted TV (aw_pocs_tv) and PICCS (piccs_tv) ----
+//
+// Both reuse the backward-difference stencil of gradientTV with two changes:
+// * AwTV (GD_AwTV.cu:117-158): every difference component d_c carries the weight
+//   w_c = exp(-(d_c / delta)^2), in the numerators and inside the norms;
+// * PICCS (PICCS.cu:117-154, :274-380) runs on the bare image (no halo slices: a z
+//   difference whose neighbour is outside is 0, like x and y) and descends along
+//   (1 - ratio) grad TV(f) + ratio grad TV(f - prior), with 1e-6 (not 1e-8) added to each norm.
+// A step is again two passes (norm, then update), with the gradient recomputed.
+
+struct TVStep {
+    const float* prior;   // PICCS prior image (same layout as f)
+    float inv_delta;      // AwTV: 1 / delta
+    float ratio;          // PICCS: weight of the prior term
+    double norm_eps;      // added to sum(g^2) before the square root
+    float grad_eps;       // added to every gradient norm: 1e-8 (GD_AwTV.cu:131), 1e-6 (PICCS.cu:149)
+};
+
+template <bool HALO, bool AW, typename Rd>
+__device__ __forceinline__ float tv_stencil(const Rd& rd, const TVDims& d, int x, int y, int z, float idl, float eps) {
+    auto val = [&](int xx, int yy, int zz) -> float { return (zz >= 0 && zz < d.nz) ? rd(xx, yy, zz) : 0.f; };
+    auto wt = [&](float v) -> float {
+        if (!AW) return 1.f;
+        const float t = v * idl;
+        return expf(-(t * t));
+    };
+    // |grad| with weights: sqrt(w0 a0^2 + w1 a1^2 + w2 a2^2) + eps
+    auto nrm = [&](float a0, float a1, float a2, float w0, float w1, float w2) {
+        return sqrtf(w0 * a0 * a0 + w1 * a1 * a1 + w2 * a2 * a2) + eps;
+    };
+    const bool zlow = HALO || z > 0;
+    const float c = val(x, y, z);
+    const float d0 = zlow ? c - val(x, y, z - 1) : 0.f;
+    const float d1 = y > 0 ? c - val(x, y - 1, z) : 0.f;
+    const float d2 = x > 0 ? c - val(x - 1, y, z) : 0.f;
+    const float w0 = wt(d0), w1 = wt(d1), w2 = wt(d2);
+    float g = (w0 * d0 + w1 * d1 + w2 * d2) / nrm(d0, d1, d2, w0, w1, w2);
+    if (x + 1 < d.nx) {   // neighbour (x+1): its x difference involves f(x)
+        const float n = val(x + 1, y, z);
+        const float e0 = zlow ? n - val(x + 1, y, z - 1) : 0.f;
+        const float e1 = y > 0 ? n - val(x + 1, y - 1, z) : 0.f;
+        const float e2 = n - c;
+        const float v2 = wt(e2);
+        g -= v2 * e2 / nrm(e0, e1, e2, wt(e0), wt(e1), v2);
+    }
+    if (y + 1 < d.ny) {
+        const float n = val(x, y + 1, z);
+        const float e0 = zlow ? n - val(x, y + 1, z - 1) : 0.f;
+        const float e1 = n - c;
+        const float e2 = x > 0 ? n - val(x - 1, y + 1, z) : 0.f;
+        const float v1 = wt(e1);
+        g -= v1 * e1 / nrm(e0, e1, e2, wt(e0), v1, wt(e2));
+    }
+    if (HALO || z + 1 < d.nz) {   // neighbour (z+1); with the halo, above the last slice it is 0
+        const float n = val(x, y, z + 1);
+        const float e0 = n - c;
+        const float e1 = y > 0 ? n - val(x, y - 1, z + 1) : 0.f;
+        const float e2 = x > 0 ? n - val(x - 1, y, z + 1) : 0.f;
+        const float v0 = wt(e0);
+        g -= v0 * e0 / nrm(e0, e1, e2, v0, wt(e1), wt(e2));
+    }
+    return g;
+}
+
+constexpr int kTvAw = 1, kTvPiccs = 2;
+
+template <int KIND>
+__device__ __forceinline__ float tv_step_grad(const float* __restrict__ f, const TVDims& d, const TVStep& s, int x,
+                                              int y, int z) {
+    auto rf = [&](int xx, int yy, int zz) { return __ldg(f + ((size_t)zz * d.ny + yy) * d.nx + xx); };
+    if (KIND == kTvAw) return tv_stencil<true, true>(rf, d, x, y, z, s.inv_delta, s.grad_eps);
+    auto rdiff = [&](int xx, int yy, int zz) {
+        const size_t i = ((size_t)zz * d.ny + yy) * d.nx + xx;
+        return __ldg(f + i) - __ldg(s.prior + i);
+    };
+    const float ga = tv_stencil<false, false>(rf, d, x, y, z, 0.f, s.grad_eps);
+    const float gb = tv_stencil<false, false>(rdiff, d, x, y, z, 0.f, s.grad_eps);
+    return fmaf(1.f - s.ratio, ga, s.ratio * gb);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(256) tv_step_norm_kernel(const float* __restrict__ f, TVDims d, TVStep st,
+                                                           double* __restrict__ out) {
+    const size_t n = (size_t)d.nx * d.ny * d.nz;
+    double s = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % d.nx);
+        const size_t r = i / d.nx;
+        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
+        const float g = tv_step_grad<KIND>(f, d, st, x, y, z);
+        s += (double)g * (double)g;
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0) atomicAdd(out, s);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(256) tv_step_update_kernel(const float* __restrict__ f, float* __restrict__ o,
+                                                             TVDims d, TVStep st, const double* __restrict__ sumsq,
+                                                             float alpha) {
+    const size_t n = (size_t)d.nx * d.ny * d.nz;
+    const float scale = (float)((double)alpha / sqrt(*sumsq + st.norm_eps));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % d.nx);
+        const size_t r = i / d.nx;
+        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
+        const float g = tv_step_grad<KIND>(f, d, st, x, y, z);
+        o[i] = fmaf(-scale, g, __ldg(f + i));
+    }
+}
+
 int grid_for(size_t n) {
     const size_t want = (n + 255) / 256;
     return (int)std::min<size_t>(want, 148 * 16);
@@ -207,6 +318,58 @@ int tigre_tv_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha
     TIGRE_CUDA(cudaGetLastError());
     note_launches(2ull * (unsigned long long)max_iter);
     return TIGRE_SUCCESS;
+}
+
+}  // extern "C"
+
+// Shared driver of the weighted / prior TV descents: ping-pong between d_img and d_work.
+template <int KIND>
+static int tv_descent(void* d_img, long nx, long ny, long nz, float alpha, int max_iter, const TVStep& stp,
+                      float* d_work, cudaStream_t st) {
+    TVDims d{(int)nx, (int)ny, (int)nz};
+    const size_t n = (size_t)nx * ny * nz;
+    double* sums = nullptr;
+    TIGRE_CUDA(cudaMallocAsync(&sums, sizeof(double) * (size_t)std::max(max_iter, 1), st));
+    TIGRE_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)std::max(max_iter, 1), st));
+    float* cur = (float*)d_img;
+    float* nxt = d_work;
+    for (int it = 0; it < max_iter; ++it) {
+        tv_step_norm_kernel<KIND><<<grid_for(n), 256, 0, st>>>(cur, d, stp, sums + it);
+        tv_step_update_kernel<KIND><<<grid_for(n), 256, 0, st>>>(cur, nxt, d, stp, sums + it, alpha);
+        std::swap(cur, nxt);
+    }
+    if (cur != (float*)d_img) TIGRE_CUDA(cudaMemcpyAsync(d_img, cur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    TIGRE_CUDA(cudaFreeAsync(sums, st));
+    TIGRE_CUDA(cudaGetLastError());
+    note_launches(2ull * (unsigned long long)max_iter);
+    return TIGRE_SUCCESS;
+}
+
+extern "C" {
+
+// In-place adaptive-weighted TV descent (aw_pocs_tv, GD_AwTV.cu:276-720): per step
+//   g = grad AwTV(f);  f <- f - alpha g / sqrt(sum g^2 + 1e-7).
+int tigre_tv_aw_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha, int max_iter, float delta,
+                    float* d_work, void* stream) {
+    if (dtype != TIGRE_F32) return fail(TIGRE_ERR_BAD_ASSERT, "TV kernels take float32 volumes");
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !d_img || !d_work || max_iter < 0)
+        return fail(TIGRE_ERR_BAD_ASSERT, "bad TV arguments");
+    if ((double)nx * ny * nz >= 2147483647.0) return fail(TIGRE_ERR_BAD_ASSERT, "volume too large");
+    if (!(delta != 0.f) || !std::isfinite(delta)) return fail(TIGRE_ERR_BAD_ASSERT, "AwTV: delta must be finite and nonzero");
+    const TVStep stp{nullptr, 1.f / delta, 0.f, 1e-7, 1e-8f};
+    return tv_descent<kTvAw>(d_img, nx, ny, nz, alpha, max_iter, stp, d_work, (cudaStream_t)stream);
+}
+
+// In-place PICCS TV descent (piccs_tv, PICCS.cu:274-380): per step
+//   g = (1 - ratio) grad TV(f) + ratio grad TV(f - prior);  f <- f - alpha g / sqrt(sum g^2).
+int tigre_tv_piccs(void* d_img, const void* d_prior, int dtype, long nx, long ny, long nz, float alpha, float ratio,
+                   int max_iter, float* d_work, void* stream) {
+    if (dtype != TIGRE_F32) return fail(TIGRE_ERR_BAD_ASSERT, "TV kernels take float32 volumes");
+    if (nx <= 0 || ny <= 0 || nz <= 0 || !d_img || !d_prior || !d_work || max_iter < 0)
+        return fail(TIGRE_ERR_BAD_ASSERT, "bad TV arguments");
+    if ((double)nx * ny * nz >= 2147483647.0) return fail(TIGRE_ERR_BAD_ASSERT, "volume too large");
+    const TVStep stp{(const float*)d_prior, 0.f, ratio, 0.0, 1e-6f};
+    return tv_descent<kTvPiccs>(d_img, nx, ny, nz, alpha, max_iter, stp, d_work, (cudaStream_t)stream);
 }
 
 }  // extern "C"

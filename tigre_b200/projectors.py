@@ -110,6 +110,30 @@ def tv_pocs_(vol: torch.Tensor, alpha: float, maxiter: int, work: torch.Tensor =
     return vol
 
 
+def tv_aw_pocs_(vol: torch.Tensor, alpha: float, maxiter: int, delta: float, work: torch.Tensor = None):
+    """In-place adaptive-weighted TV descent (aw_pocs_tv semantics) on a float32 device volume."""
+    nx, ny, nz = _vol3(vol)
+    if work is None:
+        work = torch.empty_like(vol)
+    N.check(N.lib().tigre_tv_aw_pocs(C.c_void_p(vol.data_ptr()), N.F32, nx, ny, nz, float(alpha), int(maxiter),
+                                     float(delta), C.c_void_p(work.data_ptr()), _stream(vol)), "tigre_tv_aw_pocs")
+    return vol
+
+
+def tv_piccs_(vol: torch.Tensor, prior: torch.Tensor, alpha: float, ratio: float, maxiter: int,
+              work: torch.Tensor = None):
+    """In-place PICCS TV descent (piccs_tv semantics) on a float32 device volume with a device prior."""
+    nx, ny, nz = _vol3(vol)
+    if tuple(_vol3(prior)) != (nx, ny, nz):
+        raise ValueError("prior and image sizes differ")
+    if work is None:
+        work = torch.empty_like(vol)
+    N.check(N.lib().tigre_tv_piccs(C.c_void_p(vol.data_ptr()), C.c_void_p(prior.data_ptr()), N.F32, nx, ny, nz,
+                                   float(alpha), float(ratio), int(maxiter), C.c_void_p(work.data_ptr()),
+                                   _stream(vol)), "tigre_tv_piccs")
+    return vol
+
+
 def tv_gradient(vol: torch.Tensor, out: torch.Tensor = None):
     nx, ny, nz = _vol3(vol)
     if out is None:
