@@ -137,6 +137,14 @@ int tigre_piccs_tv(const float* img, const float* prior, float* dst, float alpha
 int tigre_tvdenoising(const float* src, float* dst, float lambda, const float* spacing, const long* image_size,
                       int max_iter, const int* gpu_ids, int n_gpus);
 
+/* Poisson noise out[i] = Poisson(in[i]), plus N(mu, sigma) when gaussian != 0, on n host floats.
+ * Replaces poisson_1d / poisson_gaussian_1d (Common/CUDA/RandomNumberGenerator.hpp,
+ * RandomNumberGenerator.cu), behind tigre.utilities.CTnoise.add.  Counter-based: the result
+ * depends only on seed and element index (the reference's curand stream cannot be reproduced;
+ * the C++ compat symbols pass the reference's fixed seed 1234). */
+int tigre_noise_1d(const float* in, long long n, int gaussian, float mu, float sigma, unsigned long long seed,
+                   float* out, const int* gpu_ids, int n_gpus);
+
 /* Parallel-beam projection and backprojection.  Replace siddon_ray_projection_parallel
  * (Common/CUDA/Siddon_projection_parallel.hpp, Siddon_projection_parallel.cu:270),
  * interpolation_projection_parallel (ray_interpolated_projection_parallel.hpp,
@@ -224,6 +232,14 @@ int tigre_tv_denoise(const float* d_src, float* d_dst, long nx, long ny, long nz
 int tigre_tv_gradient(const void* d_img, int dtype, float* d_grad, long nx, long ny, long nz, void* stream);
 /* TV value sum_i |grad f_i| consistent with tigre_tv_gradient; added into *d_out (FP64). */
 int tigre_tv_value(const void* d_img, int dtype, long nx, long ny, long nz, double* d_out, void* stream);
+
+/* Device noise (same generator as tigre_noise_1d); d_in and d_out may alias. */
+int tigre_add_noise(const float* d_in, float* d_out, long long n, int gaussian, float mu, float sigma,
+                    unsigned long long seed, void* stream);
+/* Raw Philox4x32-10 blocks: d_out[4j..4j+3] = philox(counter = {j, counter_hi}, key = seed) for
+ * j < nblocks (64-bit halves little-endian); d_out 16-byte aligned.  The generator behind the noise. */
+int tigre_philox4x32(unsigned int* d_out, long long nblocks, unsigned long long counter_hi, unsigned long long seed,
+                     void* stream);
 
 /* FP64 reductions and fused CGLS updates (device scalars, no host round trip). */
 int tigre_sumsq(const void* d_x, int dtype, long n, double* d_out, void* stream);          /* *d_out += sum x^2 */

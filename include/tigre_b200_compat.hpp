@@ -10,6 +10,7 @@
 //   Common/CUDA/GD_AwTV.hpp:58                    aw_pocs_tv
 //   Common/CUDA/PICCS.hpp:58                      piccs_tv
 //   Common/CUDA/tv_proximal.hpp:52                tvdenoising
+//   Common/CUDA/RandomNumberGenerator.hpp         poisson_1d, poisson_gaussian_1d
 //   and the *_parallel symbols referenced by _Ax.pyx:21-26 / _Atb.pyx:21-22.
 //
 // `Geometry` and `GpuIds` here are declared with the field layout of
@@ -19,6 +20,8 @@
 // Include either this header or the reference's headers, never both.
 #ifndef TIGRE_B200_COMPAT_HPP
 #define TIGRE_B200_COMPAT_HPP
+
+#include <cstddef>
 
 #ifndef TYPES_CBCT
 #define TYPES_CBCT
@@ -68,6 +71,10 @@ int voxel_backprojection_parallel(float* projections, Geometry geo, float* resul
                                   int nalpha, const GpuIds& gpuids);
 // The reference returns void here; errors are reported on stderr and leave dst unchanged.
 void pocs_tv(float* img, float* dst, float alpha, const long* image_size, int maxIter, const GpuIds& gpuids);
+// Common/CUDA/RandomNumberGenerator.hpp: Poisson (+ Gaussian) noise, seed 1234 on every call.
+void poisson_1d(const float* pfIn, size_t uiLen, float* pfOut, const GpuIds& gpuids);
+void poisson_gaussian_1d(const float* pfPoissonL, size_t uiLen, float fGaussMu, float fGaussSigma, float* pfOut,
+                         GpuIds& gpuids);
 // Common/CUDA/GD_AwTV.hpp:58 and PICCS.hpp:58; void like the reference, errors on stderr.
 void aw_pocs_tv(float* img, float* dst, float alpha, const long* image_size, int maxIter, const float delta,
                 const GpuIds& gpuids);

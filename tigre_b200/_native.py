@@ -99,6 +99,11 @@ _SIGS = {
                                    C.c_void_p, C.c_void_p]),
     "tigre_tv_piccs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_float,
                                  C.c_int, C.c_void_p, C.c_void_p]),
+    "tigre_noise_1d": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.c_float, C.c_float, C.c_ulonglong, C.c_void_p,
+                                 C.c_void_p, C.c_int]),
+    "tigre_add_noise": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_float, C.c_float,
+                                  C.c_ulonglong, C.c_void_p]),
+    "tigre_philox4x32": (C.c_int, [C.c_void_p, C.c_longlong, C.c_ulonglong, C.c_ulonglong, C.c_void_p]),
     "tigre_tv_denoise_work_floats": (C.c_longlong, [C.c_long, C.c_long, C.c_long]),
     "tigre_tv_denoise": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long, C.c_long, C.c_long, C.c_float, C.c_void_p,
                                    C.c_int, C.c_void_p, C.c_void_p]),

@@ -429,6 +429,26 @@ int host_tvdenoising(const float* src, float* dst, float lambda, const float* sp
     return TIGRE_SUCCESS;
 }
 
+int host_noise(const float* in, long long n, int gaussian, float mu, float sigma, unsigned long long seed, float* out,
+               const int* ids, int ng) {
+    if (n < 0 || (n > 0 && (!in || !out))) return fail(TIGRE_ERR_BAD_ASSERT, "null argument");
+    if (n == 0) return TIGRE_SUCCESS;
+    int dev = 0;
+    if (int rc = pick_device(ids, ng, &dev)) return rc;
+    DeviceGuard g(dev);
+    DeviceState* S = state(dev);
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (int rc = S->init(dev)) return rc;
+    void *din = nullptr, *dout = nullptr;
+    if (int rc = S->get(0, (size_t)n * sizeof(float), &din)) return rc;
+    if (int rc = S->get(1, (size_t)n * sizeof(float), &dout)) return rc;
+    TIGRE_CUDA(cudaMemcpyAsync(din, in, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, S->st));
+    if (int rc = tigre_add_noise((const float*)din, (float*)dout, n, gaussian, mu, sigma, seed, S->st)) return rc;
+    TIGRE_CUDA(cudaMemcpyAsync(out, dout, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, S->st));
+    TIGRE_CUDA(cudaStreamSynchronize(S->st));
+    return TIGRE_SUCCESS;
+}
+
 }  // namespace
 
 extern "C" void tigre_release_cache(void) {
@@ -466,6 +486,11 @@ int tigre_voxel_backprojection2(const float* proj, const TigreGeometry* geo, flo
 int tigre_pocs_tv(const float* img, float* dst, float alpha, const long* image_size, int max_iter, const int* ids,
                   int n) {
     return host_pocs_tv(img, dst, alpha, image_size, max_iter, ids, n);
+}
+
+int tigre_noise_1d(const float* in, long long n, int gaussian, float mu, float sigma, unsigned long long seed,
+                   float* out, const int* ids, int ng) {
+    return host_noise(in, n, gaussian, mu, sigma, seed, out, ids, ng);
 }
 
 int tigre_aw_pocs_tv(const float* img, float* dst, float alpha, const long* image_size, int max_iter, float delta,

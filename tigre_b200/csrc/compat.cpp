@@ -69,6 +69,20 @@ void piccs_tv(const float* img, const float* prior, float* dst, float alpha, flo
     if (rc) std::fprintf(stderr, "minimizeTV:PICCS_TV: error %d: %s\n", rc, tigre_last_error());
 }
 
+// RandomNumberGenerator.hpp: the reference seeds every call with 1234 (setup_kernel), so
+// repeated calls on the same input give the same noise; so do these.
+void poisson_1d(const float* pfIn, size_t uiLen, float* pfOut, const GpuIds& ids) {
+    const int rc = tigre_noise_1d(pfIn, (long long)uiLen, 0, 0.f, 0.f, 1234ull, pfOut, ids.m_piDeviceIds, ids.m_iCount);
+    if (rc) std::fprintf(stderr, "RandomNumberGenerator: poisson_1d error %d: %s\n", rc, tigre_last_error());
+}
+
+void poisson_gaussian_1d(const float* pfPoissonL, size_t uiLen, float fGaussMu, float fGaussSigma, float* pfOut,
+                         GpuIds& ids) {
+    const int rc = tigre_noise_1d(pfPoissonL, (long long)uiLen, 1, fGaussMu, fGaussSigma, 1234ull, pfOut,
+                                  ids.m_piDeviceIds, ids.m_iCount);
+    if (rc) std::fprintf(stderr, "RandomNumberGenerator: poisson_gaussian_1d error %d: %s\n", rc, tigre_last_error());
+}
+
 void tvdenoising(float* src, float* dst, float lambda, const float* spacing, const long* image_size, int maxIter,
                  const GpuIds& ids) {
     const int rc = tigre_tvdenoising(src, dst, lambda, spacing, image_size, maxIter, ids.m_piDeviceIds, ids.m_iCount);
