@@ -340,6 +340,24 @@ def fista(proj, geo, angles, niter, hyper, tviter=20, tvlambda=0.1):
     return x.astype(np.float32)
 
 
+def mlem(proj, geo, angles, niter, x0=None):
+    """MLEM of statistical_algorithms.py:11-55 in FP64 over the oracle pair (interpolated Ax,
+    matched Atb)."""
+    b = np.asarray(proj, dtype=np.float64)
+    W = atb(np.ones(b.shape, dtype=np.float32), geo, angles, "matched").astype(np.float64)
+    W[W <= 0.0] = np.inf
+    shape = tuple(int(v) for v in geo.nVoxel)
+    x = np.ones(shape, dtype=np.float64) if x0 is None else np.array(x0, dtype=np.float64)
+    x[x < 0.0] = 0.0
+    for _ in range(niter):
+        den = ax(x.astype(np.float32), geo, angles, "interpolated").astype(np.float64)
+        den[den == 0.0] = np.inf
+        img = atb((b / den).astype(np.float32), geo, angles, "matched").astype(np.float64) / W
+        x = x * img
+        x[x < 0.0] = 0.0
+    return x.astype(np.float32)
+
+
 def lsqr(proj, geo, angles, niter):
     """LSQR of krylov_subspace_algorithms.py:101-187 with FP64 vectors over the oracle pair."""
     A = lambda v: ax(v.astype(np.float32), geo, angles, "Siddon").astype(np.float64)  # noqa: E731

@@ -177,6 +177,36 @@ def test_pocs_family_runs_and_reconstructs():
         assert np.linalg.norm(x - s * img) < 0.8 * np.linalg.norm(s * img), name
 
 
+def test_mlem_matches_oracle():
+    """MLEM (statistical_algorithms.py:11-55): interpolated Ax, matched Atb, sensitivity image,
+    multiplicative update, against the FP64 oracle restatement."""
+    import tigre_b200 as tigre
+    geo, ang, img = _case(views=24)
+    proj = O.ax(img, geo, ang, "Siddon")
+    got = tigre.algorithms.mlem(proj, geo, ang, 4)
+    ref = O.mlem(proj, geo, ang, 4)
+    mx, l2 = G.rel_err(got, ref)
+    assert mx <= 1e-4 and l2 <= 1e-5, (mx, l2)
+    x, res = tigre.algorithms.mlem(proj, geo, ang, 6, computel2=True)
+    assert res.shape == (1, 6) and np.all(np.diff(res[0]) < 0)
+
+
+@pytest.mark.parametrize("name", ["sart_tv", "ossart_tv"])
+def test_sart_tv_first_iteration_matches_oracle_denoiser(name):
+    """SART_TV / OSSART_TV (art_family_algorithms.py:65-152): one sweep, then im3ddenoise with
+    the reference's tvlambda / tviter, against the oracle denoiser applied to the same sweep."""
+    import tigre_b200 as tigre
+    geo, ang, proj = _noisy_case()
+    os_ = name == "ossart_tv"
+    sweep = (tigre.algorithms.ossart(proj, geo, ang, 1, blocksize=5) if os_ else
+             tigre.algorithms.sart(proj, geo, ang, 1))
+    kw = {"blocksize": 5} if os_ else {}
+    got = getattr(tigre.algorithms, name)(proj, geo, ang, 1, tviter=20, tvlambda=30, **kw)
+    ref = O.im3ddenoise(sweep, 20, 30)
+    mx, l2 = G.rel_err(got, ref)
+    assert mx <= 1e-5 and l2 <= 1e-6, (name, mx, l2)
+
+
 def test_autograd_backward_is_matched_adjoint():
     import torch
     from tigre_b200 import autograd as AG, projectors as P

@@ -146,3 +146,38 @@ def sirt(proj, geo, angles, niter, **kwargs):
 def sart(proj, geo, angles, niter, **kwargs):
     kwargs.pop("blocksize", None)
     return _run(proj, geo, angles, niter, 1, kwargs)
+
+
+def _run_tv(proj, geo, angles, niter, blocksize, kwargs):
+    """SART_TV / OSSART_TV (art_family_algorithms.py:65-152): per iteration one (OS-)SART sweep,
+    then im3ddenoise(res, tviter, tvlambda) (TV proximal operator on the device)."""
+    from ..utilities.im_3d_denoise import im3ddenoise
+    prob = Problem(proj, geo, angles, kwargs.get("gpuids"))
+    art = ART(prob, blocksize, kwargs.get("OrderStrategy"), kwargs.get("lmbda", 1.0), kwargs.get("noneg", True), None,
+              kwargs.get("verbose", False))
+    tvlambda = kwargs.get("tvlambda", 50)
+    tviter = kwargs.get("tviter", 50)
+    init = kwargs.get("init", None)
+    if isinstance(init, str) and init == "FDK":
+        from .single_pass import fdk_device
+        x = fdk_device(prob).clamp_(min=0)
+    elif init is not None and not isinstance(init, str):
+        x = prob.to_device_vol(init)
+    else:
+        x = prob.zeros_vol()
+    for _ in range(niter):
+        art.sweep(x)
+        x = im3ddenoise(x, tviter, tvlambda).contiguous()
+    return prob.out(x)
+
+
+def sart_tv(proj, geo, angles, niter, **kwargs):
+    """Drop-in for tigre.algorithms.sart_tv (blocksize 1, tvlambda 50, tviter 50)."""
+    if kwargs.get("blocksize", 1) > 1:
+        print("Warning: blocksize is set to 1, please use an OS version of the algorithm for blocksize > 1")
+    return _run_tv(proj, geo, angles, niter, 1, kwargs)
+
+
+def ossart_tv(proj, geo, angles, niter, **kwargs):
+    """Drop-in for tigre.algorithms.ossart_tv (blocksize default 20, tvlambda 50, tviter 50)."""
+    return _run_tv(proj, geo, angles, niter, kwargs.get("blocksize", 20), kwargs)
