@@ -358,6 +358,214 @@ def mlem(proj, geo, angles, niter, x0=None):
     return x.astype(np.float32)
 
 
+def _kry_ops(geo, angles):
+    A = lambda v: ax(np.asarray(v, dtype=np.float32), geo, angles, "Siddon").astype(np.float64)  # noqa: E731
+    At = lambda r: atb(np.asarray(r, dtype=np.float32), geo, angles, "matched").astype(np.float64)  # noqa: E731
+    return A, At
+
+
+def _kry_stop(i, l2, restart):
+    return i > 0 and l2[i] > l2[i - 1] and (i == 1 or not restart)
+
+
+def hybrid_lsqr(proj, geo, angles, niter, lmbda=1.0, restart=True):
+    """hybrid_LSQR of krylov_subspace_algorithms.py:190-296 in FP64 (elementwise
+    re-orthogonalisation kept); returns the last non-growing iterate."""
+    A, At = _kry_ops(geo, angles)
+    b = np.asarray(proj, dtype=np.float64)
+    x = np.zeros(tuple(int(v) for v in geo.nVoxel))
+    u = b - A(x)
+    normr = np.linalg.norm(u)
+    u = u / normr
+    U, V = [u], []
+    B = np.zeros((niter, niter + 1))
+    rhs = np.zeros(niter + 1)
+    rhs[0] = normr
+    beta = normr
+    l2, best = [], x
+    for i in range(niter):
+        v = At(u)
+        if i > 0:
+            v = v - beta * V[i - 1]
+        for j in range(i - 1):
+            v = v - V[j] * v * V[j]
+        alpha = np.linalg.norm(v)
+        v = v / alpha
+        V.append(v)
+        u = A(v) - alpha * u
+        for j in range(i - 1):
+            u = u - U[j] * u * U[j]
+        beta = np.linalg.norm(u)
+        u = u / beta
+        U.append(u)
+        B[i, i], B[i, i + 1] = alpha, beta
+        Uk, Sk, Vh = np.linalg.svd(B[:i + 1, :i + 2].T)
+        y = Vh.T @ (Sk * (Uk.T @ rhs[:i + 2])[:i + 1] / (Sk ** 2 + lmbda ** 2))
+        xi = x + sum(V[j] * y[j] for j in range(i + 1))
+        l2.append(np.linalg.norm(b - A(xi)))
+        if _kry_stop(i, l2, restart):
+            return best.astype(np.float32), np.asarray(l2[:-1])
+        best = xi
+    return best.astype(np.float32), np.asarray(l2)
+
+
+def gmres(proj, geo, angles, niter, space, restart=True):
+    """AB-GMRES (space='proj', :570-631) / BA-GMRES (space='vol', :634-695) with the matched
+    backprojector, in FP64."""
+    A, At = _kry_ops(geo, angles)
+    b = np.asarray(proj, dtype=np.float64)
+    x = np.zeros(tuple(int(v) for v in geo.nVoxel))
+    r = b - A(x)
+    if space == "vol":
+        r = At(r)
+    rn = np.linalg.norm(r)
+    W = [r / rn]
+    H = np.zeros((niter, niter + 1))
+    l2, best = [], x
+    for k in range(niter):
+        q = A(At(W[k])) if space == "proj" else At(A(W[k]))
+        for i in range(k + 1):
+            H[k, i] = np.sum(q * W[i])
+            q = q - H[k, i] * W[i]
+        H[k, k + 1] = np.linalg.norm(q)
+        W.append(q / H[k, k + 1])
+        e1 = np.zeros(k + 2)
+        e1[0] = rn
+        y = np.linalg.lstsq(H[:k + 1, :k + 2].T, e1, rcond=None)[0]
+        d = sum(W[i] * y[i] for i in range(k + 1))
+        xi = x + (At(d) if space == "proj" else d)
+        l2.append(np.linalg.norm(b - A(xi)))
+        if _kry_stop(k, l2, restart):
+            return best.astype(np.float32), np.asarray(l2[:-1])
+        best = xi
+    return best.astype(np.float32), np.asarray(l2)
+
+
+def _irn_diffs(img):
+    out = []
+    for axis in range(3):
+        d = img.copy()
+        n = img.shape[axis]
+        sl = [slice(None)] * 3
+        lo, hi = list(sl), list(sl)
+        lo[axis], hi[axis] = slice(0, n - 2), slice(1, n - 1)
+        if n > 2:
+            d[tuple(lo)] = img[tuple(lo)] - img[tuple(hi)]
+        out.append(d)
+    return out
+
+
+def _irn_Lx(W, img):
+    return np.stack([W * d for d in _irn_diffs(img)])
+
+
+def _irn_Ltx(W, g3):
+    acc = 0.0
+    for axis in range(3):
+        wg = W * g3[axis]
+        o = wg.copy()
+        n = wg.shape[axis]
+        idx = lambda a, b_: tuple(slice(a, b_) if k == axis else slice(None) for k in range(3))  # noqa: E731
+        if n > 3:
+            o[idx(1, n - 2)] = wg[idx(1, n - 2)] - wg[idx(0, n - 3)]
+        if n >= 2:
+            o[idx(n - 1, n)] = -wg[idx(n - 2, n - 1)]
+        acc = acc + o
+    return acc
+
+
+def irn_tv_cgls(proj, geo, angles, niter, lmbda=1.0, niter_outer=4):
+    """IRN_TV_CGLS of krylov_subspace_algorithms.py:441-567 in FP64, with the reference's
+    difference operators (:466-500) and its restart-from-res0 bookkeeping."""
+    A, At = _kry_ops(geo, angles)
+    b = np.asarray(proj, dtype=np.float64)
+    sl = np.sqrt(lmbda)
+    x = np.zeros(tuple(int(v) for v in geo.nVoxel))
+    x0 = x
+    l2 = []
+    for _ in range(niter_outer):
+        d = _irn_diffs(x)
+        W = (d[0] ** 2 + d[1] ** 2 + d[2] ** 2 + 1e-6) ** (-0.25)
+        x = x0
+        r1 = b - A(x)
+        r2 = -_irn_Lx(W, x) * sl
+        p = At(r1) + sl * _irn_Ltx(W, r2)
+        gamma = np.sum(p * p)
+        for _i in range(niter):
+            x0 = x
+            q1 = A(p)
+            q2 = _irn_Lx(W, p) * sl
+            alpha = gamma / (np.sum(q1 * q1) + np.sum(q2 * q2))
+            x = x + alpha * p
+            l2.append(np.linalg.norm(b - A(x)))
+            r1 = r1 - alpha * q1
+            r2 = r2 - alpha * q2
+            s_ = At(r1) + sl * _irn_Ltx(W, r2)
+            gamma1 = np.sum(s_ * s_)
+            p = s_ + gamma1 / gamma * p
+            gamma = gamma1
+    return x.astype(np.float32), np.asarray(l2)
+
+
+def hybrid_flsqr_tv(proj, geo, angles, niter, lmbda=1.0, restart=True):
+    """hybrid_fLSQR_TV of krylov_subspace_algorithms.py:698-858 in FP64, with the inner
+    scipy.sparse.linalg.lsqr solves (iter_lim=50) the reference makes; returns the iterate (the
+    reference computes it and its decorator discards it)."""
+    from scipy.sparse.linalg import LinearOperator, lsqr as sp_lsqr
+    A, At = _kry_ops(geo, angles)
+    b = np.asarray(proj, dtype=np.float64)
+    shape = tuple(int(v) for v in geo.nVoxel)
+    N = int(np.prod(shape))
+    x = np.zeros(shape)
+    u = b - A(x)
+    k_aux = A(np.ones(shape) / np.sqrt(N))
+    kn2 = np.sum(k_aux * k_aux)
+    xA0 = np.ones(shape) * (np.sum(k_aux * u) / (np.sqrt(N) * kn2))
+    k_aux = At(k_aux) / (np.sqrt(N) * kn2)
+    u = u - A(xA0)
+    normr = np.linalg.norm(u)
+    u = u / normr
+    U, V, Z = [u], [], []
+    M = np.zeros((niter, niter + 1))
+    rhs = np.zeros(niter + 1)
+    rhs[0] = normr
+    W = np.ones(shape) if x.max() == 0 else None
+    Lx = lambda t: _irn_Lx(W, t.reshape(shape)).ravel()  # noqa: E731
+    Ltx = lambda t: _irn_Ltx(W, t.reshape((3,) + shape)).ravel()  # noqa: E731
+    l2, best = [], x + xA0
+    for i in range(niter):
+        v = At(u)
+        for j in range(i):
+            v = v - np.sum(V[j] * v) * V[j]
+        v = v / np.linalg.norm(v)
+        zt = v.ravel() - k_aux.ravel() * np.sum(v)
+        op1 = LinearOperator((N, 3 * N), matvec=Ltx, rmatvec=Lx, dtype=np.float64)
+        aux = sp_lsqr(op1, zt, iter_lim=50)[0]
+        op2 = LinearOperator((3 * N, N), matvec=Lx, rmatvec=Ltx, dtype=np.float64)
+        zt = sp_lsqr(op2, aux, iter_lim=50)[0]
+        zt = (zt - np.sum(k_aux.ravel() * zt)).reshape(shape)
+        V.append(v)
+        Z.append(zt)
+        u = A(zt)
+        for j in range(i + 1):
+            M[i, j] = np.sum(U[j] * u)
+            u = u - M[i, j] * U[j]
+        M[i, i + 1] = np.linalg.norm(u)
+        u = u / M[i, i + 1]
+        U.append(u)
+        WZ = np.stack([Lx(Z[j]) for j in range(i + 1)], axis=1)
+        R = np.linalg.qr(WZ, mode="r")
+        MZ = np.concatenate([M[:i + 1, :i + 2].T, lmbda * R])
+        rz = np.concatenate([rhs[:i + 2], np.zeros(i + 1)])
+        y = np.linalg.lstsq(MZ, rz, rcond=None)[0]
+        xi = x + xA0 + sum(Z[j] * y[j] for j in range(i + 1))
+        l2.append(np.linalg.norm(b - A(xi)))
+        if _kry_stop(i, l2, restart):
+            return best.astype(np.float32), np.asarray(l2[:-1])
+        best = xi
+    return best.astype(np.float32), np.asarray(l2)
+
+
 def lsqr(proj, geo, angles, niter):
     """LSQR of krylov_subspace_algorithms.py:101-187 with FP64 vectors over the oracle pair."""
     A = lambda v: ax(v.astype(np.float32), geo, angles, "Siddon").astype(np.float64)  # noqa: E731

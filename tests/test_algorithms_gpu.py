@@ -207,6 +207,51 @@ def test_sart_tv_first_iteration_matches_oracle_denoiser(name):
     assert mx <= 1e-5 and l2 <= 1e-6, (name, mx, l2)
 
 
+@pytest.mark.parametrize("name", ["hybrid_lsqr", "ab_gmres", "ba_gmres", "irn_tv_cgls"])
+def test_krylov_extensions_match_oracle(name):
+    """hybrid LSQR, AB-/BA-GMRES (matched backprojector), IRN-TV-CGLS against their FP64
+    restatements over the oracle pair."""
+    import tigre_b200 as tigre
+    geo, ang, img = _case(views=24)
+    proj = O.ax(img, geo, ang, "Siddon")
+    if name == "hybrid_lsqr":
+        ref, rl2 = O.hybrid_lsqr(proj, geo, ang, 6)
+    elif name == "irn_tv_cgls":
+        ref, rl2 = O.irn_tv_cgls(proj, geo, ang, 3, niter_outer=2)
+    else:
+        ref, rl2 = O.gmres(proj, geo, ang, 6, "proj" if name == "ab_gmres" else "vol")
+    kw = {"niter_outer": 2} if name == "irn_tv_cgls" else {}
+    n = 3 if name == "irn_tv_cgls" else 6
+    got, l2 = getattr(tigre.algorithms, name)(proj, geo, ang, n, computel2=True, **kw)
+    mx, e2 = G.rel_err(got, ref)
+    assert mx <= 1e-3 and e2 <= 1e-4, (name, mx, e2)
+    assert l2.shape[1] == len(rl2) and np.allclose(l2[0], rl2, rtol=1e-4), (l2, rl2)
+    assert rl2[-1] < 0.5 * np.linalg.norm(proj)
+
+
+def test_hybrid_flsqr_tv_matches_oracle():
+    """hybrid fLSQR-TV against its FP64 restatement with scipy's LSQR for the inner solves."""
+    import tigre_b200 as tigre
+    geo, ang, img = _case(n=24, views=20)
+    proj = O.ax(img, geo, ang, "Siddon")
+    ref, rl2 = O.hybrid_flsqr_tv(proj, geo, ang, 4)
+    got, l2 = tigre.algorithms.hybrid_flsqr_tv(proj, geo, ang, 4, computel2=True)
+    mx, e2 = G.rel_err(got, ref)
+    assert mx <= 1e-2 and e2 <= 1e-3, (mx, e2)
+    assert np.allclose(l2[0], rl2, rtol=1e-3), (l2, rl2)
+    assert rl2[-1] < 0.5 * np.linalg.norm(proj)
+
+
+def test_gmres_fdk_backprojector_runs():
+    import tigre_b200 as tigre
+    geo, ang, img = _case(views=24)
+    proj = O.ax(img, geo, ang, "Siddon")
+    for name in ("ab_gmres", "ba_gmres"):
+        x = getattr(tigre.algorithms, name)(proj, geo, ang, 4, backprojector="FDK")
+        assert np.isfinite(x).all()
+        assert np.linalg.norm(O.ax(x, geo, ang, "Siddon") - proj) < 0.5 * np.linalg.norm(proj), name
+
+
 def test_autograd_backward_is_matched_adjoint():
     import torch
     from tigre_b200 import autograd as AG, projectors as P

@@ -56,12 +56,13 @@ def _wang(proj, geo):
     return (zproj * w * 2).astype(np.float32), zgeo
 
 
-def fdk_device(prob: Problem, filter=None, parker=False, out=None):  # noqa: A002
-    """FDK of the Problem's projections; returns a device volume."""
+def fdk_device(prob: Problem, filter=None, parker=False, out=None, proj=None):  # noqa: A002
+    """FDK of the Problem's projections (or of `proj`, a device stack of the same geometry);
+    returns a device volume."""
     T = torch()
     g = prob.geo
     w = F.cosine_weights(g, device=prob.device)
-    pw = prob.b * w
+    pw = (prob.b if proj is None else proj) * w
     aw = None
     if parker:
         W = T.from_numpy(F.parker_weights(g, prob.angles, 1.0 if parker is True else float(parker))).to(prob.device)
