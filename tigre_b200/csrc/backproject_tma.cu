@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(TXY* TXY, 2) bp_tma_kernel(const __grid_consta
             float wcol = 1.f, cu2 = 0.f, cxy = 0.f;
             if (!MATCHED) {
                 const float den = fmaf((float)y, F.wy, fmaf((float)x, F.wx, F.w0));
-                const float r = F.dso / den;
+                const float r = __fdividef(F.dso, den);
                 wcol = r * r;
             } else {
                 const float rvx = fmaf((float)x, F.dvx, F.rv0x), rvy = fmaf((float)y, F.dvy, F.rv0y);
@@ -268,7 +268,9 @@ __global__ void __launch_bounds__(TXY* TXY, 2) bp_tma_kernel(const __grid_consta
                     // so w is interpolated by the cubic through its exact values at the four
                     // Chebyshev nodes of [0, VZ-1] (relative error ~1e-7 at a 6:10 source/detector
                     // distance ratio, far below that at the usual ones).  In s = k - (VZ-1)/2,
-                    // with nodes +-na, +-nb, the cubic is e0 + o1 s + e2 s^2 + o3 s^3.
+                    // with nodes +-na, +-nb, the cubic is e0 + o1 s + e2 s^2 + o3 s^3.  The node
+                    // values use the hardware reciprocal square root and the approximate
+                    // division (each within 2 ulp), since they run once per column and view.
                     float2 c0 = f2(0.f), c1 = f2(0.f), c2 = f2(0.f), c3 = f2(0.f);
                     if (MATCHED) {
                         constexpr float hw = 0.5f * (float)(VZ - 1);
@@ -279,12 +281,12 @@ __global__ void __launch_bounds__(TXY* TXY, 2) bp_tma_kernel(const __grid_consta
                         auto wexact = [&](float kf) {
                             const float vt = fmaf(kf, vstep, vt0), dz = fmaf(vt, F.ddv, F.dzc), L2 = fmaf(dz, dz, cu2);
                             const float rvz = fmaf(kf, p.dVZ, rz0), lsq = fmaf(rvz, rvz, cxy);
-                            return L2 * sqrtf(L2) / (F.dsd * lsq);
+                            return __fdividef(L2 * L2 * rsqrtf(L2), F.dsd * lsq);
                         };
                         const float wpa = wexact(hw + na), wma = wexact(hw - na);
                         const float wpb = wexact(hw + nb), wmb = wexact(hw - nb);
                         const float Ea = 0.5f * (wpa + wma), Eb = 0.5f * (wpb + wmb);
-                        const float Oa = 0.5f * (wpa - wma) / na, Ob = 0.5f * (wpb - wmb) / nb;
+                        const float Oa = (wpa - wma) * (0.5f / na), Ob = (wpb - wmb) * (0.5f / nb);
                         const float e2 = (Ea - Eb) * inv, o3 = (Oa - Ob) * inv;
                         c0 = f2(fmaf(-e2, na * na, Ea));
                         c1 = f2(fmaf(-o3, na * na, Oa));
