@@ -241,6 +241,18 @@ int tigre_add_noise(const float* d_in, float* d_out, long long n, int gaussian, 
 int tigre_philox4x32(unsigned int* d_out, long long nblocks, unsigned long long counter_hi, unsigned long long seed,
                      void* stream);
 
+/* 3x3x3 convolutions of the learned CGLS warm start (no reference counterpart): BF16
+ * channels-last activations x[D][H][W][C], weights w[Cout][27*Cin] (tap (dz*3+dy)*3+dx major,
+ * channel minor), zero padding 1, FP32 accumulation on the tensor cores.  d_col: scratch of
+ * tigre_conv3d_col_elems(D, H, W, Cin) BF16 elements (d_dcol: as many floats). */
+long long tigre_conv3d_col_elems(long D, long H, long W, long C);
+int tigre_conv3d_fwd(const void* d_x, const void* d_w, const float* d_bias, void* d_y_bf16, float* d_y_f32, long D,
+                     long H, long W, long Cin, long Cout, int relu, void* d_col, void* stream);
+int tigre_conv3d_bwd_data(const void* d_dy, const void* d_w, float* d_dx, long D, long H, long W, long Cin, long Cout,
+                          float* d_dcol, void* stream);
+int tigre_conv3d_bwd_weight(const void* d_x, const void* d_dy, float* d_dw, long D, long H, long W, long Cin,
+                            long Cout, void* d_col, void* stream);
+
 /* FP64 reductions and fused CGLS updates (device scalars, no host round trip). */
 int tigre_sumsq(const void* d_x, int dtype, long n, double* d_out, void* stream);          /* *d_out += sum x^2 */
 int tigre_dot(const float* d_x, const float* d_y, long n, double* d_out, void* stream);    /* *d_out += sum x*y */

@@ -1,0 +1,121 @@
+"""Learned warm start: the BF16 tensor-core 3x3x3 convolutions against PyTorch's FP32
+convolution on the CPU (forward, data gradient, weight gradient), and a small end-to-end run
+(data from the library's own projector, noise and CGLS; U-Net training; warm-started CGLS)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16_round(a):
+    import torch
+    return torch.from_numpy(np.asarray(a, dtype=np.float32)).to(torch.bfloat16).float()
+
+
+def _ref_weights(w, cin, cout):
+    """(Cout, 27*Cin) with tap (dz*3+dy)*3+dx major -> (Cout, Cin, 3, 3, 3) for F.conv3d."""
+    return w.view(cout, 27, cin).permute(0, 2, 1).reshape(cout, cin, 3, 3, 3)
+
+
+@pytest.mark.parametrize("shape,cin,cout", [((6, 5, 7), 3, 5), ((20, 16, 16), 40, 70), ((8, 8, 8), 1, 16),
+                                            ((4, 9, 6), 48, 1)])
+def test_conv3d_matches_torch_fp32(shape, cin, cout):
+    import torch
+    import torch.nn.functional as F
+    from tigre_b200 import _native as N
+    D, H, W = shape
+    rng = np.random.default_rng(cin * 7 + cout)
+    x = _bf16_round(rng.standard_normal((D, H, W, cin)))
+    w = _bf16_round(rng.standard_normal((cout, 27 * cin)) / np.sqrt(27 * cin))
+    b = torch.from_numpy(rng.standard_normal(cout).astype(np.float32))
+    dy = _bf16_round(rng.standard_normal((D, H, W, cout)))
+    # CPU FP32 reference
+    xr = x.permute(3, 0, 1, 2).unsqueeze(0).clone().requires_grad_(True)
+    wr = _ref_weights(w, cin, cout).clone().requires_grad_(True)
+    yr = F.conv3d(xr, wr, b, padding=1)
+    yr.backward(dy.permute(3, 0, 1, 2).unsqueeze(0))
+    y_ref = yr.detach()[0].permute(1, 2, 3, 0).numpy()
+    dx_ref = xr.grad[0].permute(1, 2, 3, 0).numpy()
+    dw_ref = wr.grad.permute(0, 2, 3, 4, 1).reshape(cout, 27 * cin).numpy()
+    # device
+    L = N.lib()
+    xd = x.to(torch.bfloat16).cuda()
+    wd = w.to(torch.bfloat16).cuda()
+    bd = b.cuda()
+    dyd = dy.to(torch.bfloat16).cuda()
+    col = torch.empty(int(L.tigre_conv3d_col_elems(D, H, W, cin)), dtype=torch.bfloat16, device="cuda")
+    dcol = torch.empty(int(L.tigre_conv3d_col_elems(D, H, W, cin)), dtype=torch.float32, device="cuda")
+    y = torch.empty((D, H, W, cout), dtype=torch.float32, device="cuda")
+    dx = torch.empty((D, H, W, cin), dtype=torch.float32, device="cuda")
+    dw = torch.zeros((cout, 27 * cin), dtype=torch.float32, device="cuda")
+    p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    N.check(L.tigre_conv3d_fwd(p(xd), p(wd), p(bd), None, p(y), D, H, W, cin, cout, 0, p(col), None), "fwd")
+    N.check(L.tigre_conv3d_bwd_data(p(dyd), p(wd), p(dx), D, H, W, cin, cout, p(dcol), None), "data")
+    N.check(L.tigre_conv3d_bwd_weight(p(xd), p(dyd), p(dw), D, H, W, cin, cout, p(col), None), "weight")
+    torch.cuda.synchronize()
+    for got, ref, name in ((y, y_ref, "y"), (dx, dx_ref, "dx"), (dw, dw_ref, "dw")):
+        got = got.cpu().numpy()
+        # same BF16 operands, FP32 sums in another order (tensor-core accumulation): 2e-4 of the max
+        err = np.max(np.abs(got - ref)) / max(np.max(np.abs(ref)), 1e-30)
+        assert err <= 2e-4, (name, err)
+
+
+def test_conv_autograd_matches_torch_fp32():
+    """The autograd Function (implicit-GEMM forward, flipped-weight data gradient, im2col weight
+    gradient) against F.conv3d on the CPU, with Cin and Cout multiples of 8 and not."""
+    import torch
+    import torch.nn.functional as F
+    from tigre_b200 import warmstart as WS
+    for (D, H, W), cin, cout in [((8, 6, 10), 16, 24), ((5, 7, 6), 8, 1), ((4, 4, 4), 1, 8)]:
+        rng = np.random.default_rng(cin + cout)
+        x = _bf16_round(rng.standard_normal((D, H, W, cin)))
+        w = _bf16_round(rng.standard_normal((cout, 27 * cin)) / np.sqrt(27 * cin))
+        b = torch.from_numpy(rng.standard_normal(cout).astype(np.float32))
+        dy = _bf16_round(rng.standard_normal((D, H, W, cout)))
+        xd = x.to(torch.bfloat16).cuda().requires_grad_(True)
+        wd = w.cuda().requires_grad_(True)
+        bd = b.cuda().requires_grad_(True)
+        y = WS.conv3d(xd, wd, bd, False)
+        y.backward(dy.to(torch.bfloat16).cuda())
+        xr = x.permute(3, 0, 1, 2).unsqueeze(0).clone().requires_grad_(True)
+        wr = _ref_weights(w, cin, cout).clone().requires_grad_(True)
+        br = b.clone().requires_grad_(True)
+        yr = F.conv3d(xr, wr, br, padding=1)
+        yr.backward(dy.permute(3, 0, 1, 2).unsqueeze(0))
+        pairs = [(y.float().cpu(), yr.detach()[0].permute(1, 2, 3, 0), 1e-2),            # BF16 output
+                 (xd.grad.float().cpu(), xr.grad[0].permute(1, 2, 3, 0), 1e-2),        # BF16 gradient
+                 (wd.grad.cpu(), wr.grad.permute(0, 2, 3, 4, 1).reshape(cout, 27 * cin), 2e-4),
+                 (bd.grad.cpu(), br.grad, 1e-5)]
+        for got, ref, tol in pairs:
+            err = float((got - ref).abs().max() / ref.abs().max().clamp_min(1e-30))
+            assert err <= tol, ((D, H, W), cin, cout, err, tol)
+
+
+def test_conv3d_relu_bias_and_bf16_output():
+    import torch
+    from tigre_b200 import warmstart as WS
+    rng = np.random.default_rng(3)
+    x = torch.from_numpy(rng.standard_normal((8, 8, 8, 4)).astype(np.float32)).to(torch.bfloat16).cuda()
+    w = torch.from_numpy((rng.standard_normal((6, 108)) / 10).astype(np.float32)).cuda()
+    b = torch.from_numpy(rng.standard_normal(6).astype(np.float32)).cuda()
+    y = WS.conv3d(x, w, b, True)
+    y0 = WS.conv3d(x, w, b, False)
+    assert y.dtype == torch.bfloat16 and (y >= 0).all()
+    assert torch.equal(y, torch.clamp(y0, min=0))
+
+
+def test_warmstart_end_to_end_small():
+    """32^3: training lowers the loss, the warm start is a valid CGLS start and reaches the
+    residual target; timings are reported, not asserted."""
+    import torch
+    from tigre_b200 import warmstart as WS
+    model = WS.unet(base=8, levels=3)
+    tr = WS.train(model, n_train=6, steps=40, n=32, crop=0, lr=2e-3)
+    assert tr["loss_last"] < tr["loss_first"]
+    ev = WS.evaluate(model, n_eval=2, n=32)
+    for row in ev["cases"]:
+        assert row["plain_zero"]["reached"] and row["warm"]["reached"]
+    assert np.isfinite(ev["warm_over_plain_zero"])
+    del torch

@@ -104,6 +104,13 @@ _SIGS = {
     "tigre_add_noise": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_float, C.c_float,
                                   C.c_ulonglong, C.c_void_p]),
     "tigre_philox4x32": (C.c_int, [C.c_void_p, C.c_longlong, C.c_ulonglong, C.c_ulonglong, C.c_void_p]),
+    "tigre_conv3d_col_elems": (C.c_longlong, [C.c_long, C.c_long, C.c_long, C.c_long]),
+    "tigre_conv3d_fwd": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_long,
+                                   C.c_long, C.c_long, C.c_long, C.c_int, C.c_void_p, C.c_void_p]),
+    "tigre_conv3d_bwd_data": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_long, C.c_long, C.c_long,
+                                        C.c_long, C.c_void_p, C.c_void_p]),
+    "tigre_conv3d_bwd_weight": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_long, C.c_long, C.c_long,
+                                          C.c_long, C.c_void_p, C.c_void_p]),
     "tigre_tv_denoise_work_floats": (C.c_longlong, [C.c_long, C.c_long, C.c_long]),
     "tigre_tv_denoise": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long, C.c_long, C.c_long, C.c_float, C.c_void_p,
                                    C.c_int, C.c_void_p, C.c_void_p]),

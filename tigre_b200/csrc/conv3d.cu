@@ -1,0 +1,339 @@
+// 3x3x3 convolutions for the learned CGLS warm start: BF16 operands, FP32 accumulation on
+// the tensor cores, sm_100a.
+//
+// Activations are channels-last volumes x[D][H][W][C] (BF16); weights w[Cout][27*Cin] with
+// the tap index t = (dz*3 + dy)*3 + dx major and the input channel minor; zero padding of 1,
+// stride 1.  Each convolution is an implicit GEMM done in two steps:
+//   im2col:   col[v][t*Cin + c] = x at voxel v shifted by tap t      (M = D*H*W rows, K = 27*Cin)
+//   forward:  y[v][co]  = relu?(sum_k col[v][k] w[co][k] + b[co])   (M x N = Cout, K)
+//   data:     dcol[v][k] = sum_co dy[v][co] w[co][k];  dx = col2im(dcol) (gather over taps)
+//   weight:   dw[co][k] += sum_v dy[v][co] col[v][k]                 (split over v, FP32 atomics)
+// The GEMM stages 64 x 64 output tiles through shared memory in K steps of 32 and runs them on
+// 16 x 16 x 16 BF16 warp MMA tiles (8 warps, each a 16 x 32 strip), zero-filling ragged edges,
+// so any M, N, K work.  This is the warp-level (mma.sync) tensor-core path; moving the GEMM to
+// tcgen05 with TMEM accumulators is the next step for this part.
+
+#include <cuda_bf16.h>
+#include <mma.h>
+
+#include <cstdint>
+
+#include "tigre_internal.h"
+
+namespace tigre {
+namespace {
+
+using namespace nvcuda;
+
+constexpr int kBM = 64, kBN = 64, kBK = 32;   // block tile
+constexpr int kThreads = 256;                  // 8 warps: 4 (M) x 2 (N), each 16 x 32
+
+// Element (i, k) of op(A) (M x K) and (k, j) of op(B) (K x N).
+//   A_ROW: A is row-major M x K (lda = row stride); else A is stored K x M row-major, i.e.
+//          element (i, k) at A[k * lda + i].
+//   B_COL: B is stored N x K row-major (element (k, j) at B[j * ldb + k]); else B is K x N
+//          row-major (element (k, j) at B[k * ldb + j]).
+template <bool A_ROW, bool B_COL>
+__global__ void __launch_bounds__(kThreads) gemm_kernel(const __nv_bfloat16* __restrict__ A, int lda,
+                                                        const __nv_bfloat16* __restrict__ B, int ldb, float* Cf,
+                                                        __nv_bfloat16* Cb, int ldc, int M, int N, int K,
+                                                        const float* __restrict__ bias, int relu, int k_chunk,
+                                                        int atomic) {
+    __shared__ __align__(32) __nv_bfloat16 sA[kBM][kBK + 8];
+    __shared__ __align__(32) __nv_bfloat16 sB[kBK][kBN + 8];
+    __shared__ __align__(32) float sC[kBM][kBN + 4];
+    const int tid = threadIdx.x, wid = tid >> 5;
+    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+    const int kb = blockIdx.z * k_chunk, ke = min(K, kb + k_chunk);
+    const int wm = (wid & 3) * 16, wn = (wid >> 2) * 32;
+    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[2];
+    wmma::fill_fragment(acc[0], 0.f);
+    wmma::fill_fragment(acc[1], 0.f);
+    const __nv_bfloat16 zero = __float2bfloat16(0.f);
+    for (int k0 = kb; k0 < ke; k0 += kBK) {
+        // stage A (64 x 32) and B (32 x 64), zero outside the matrices / the K chunk
+        for (int e = tid; e < kBM * kBK; e += kThreads) {
+            const int i = e / kBK, k = e % kBK;
+            const int gi = m0 + i, gk = k0 + k;
+            __nv_bfloat16 v = zero;
+            if (gi < M && gk < ke) v = A_ROW ? A[(size_t)gi * lda + gk] : A[(size_t)gk * lda + gi];
+            sA[i][k] = v;
+        }
+        for (int e = tid; e < kBK * kBN; e += kThreads) {
+            const int k = e / kBN, j = e % kBN;
+            const int gk = k0 + k, gj = n0 + j;
+            __nv_bfloat16 v = zero;
+            if (gj < N && gk < ke) v = B_COL ? B[(size_t)gj * ldb + gk] : B[(size_t)gk * ldb + gj];
+            sB[k][j] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kBK; kk += 16) {
+            wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> fa;
+            wmma::load_matrix_sync(fa, &sA[wm][kk], kBK + 8);
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> fb;
+                wmma::load_matrix_sync(fb, &sB[kk][wn + 16 * t], kBN + 8);
+                wmma::mma_sync(acc[t], fa, fb, acc[t]);
+            }
+        }
+        __syncthreads();
+    }
+    wmma::store_matrix_sync(&sC[wm][wn], acc[0], kBN + 4, wmma::mem_row_major);
+    wmma::store_matrix_sync(&sC[wm][wn + 16], acc[1], kBN + 4, wmma::mem_row_major);
+    __syncthreads();
+    for (int e = tid; e < kBM * kBN; e += kThreads) {
+        const int i = e / kBN, j = e % kBN;
+        const int gi = m0 + i, gj = n0 + j;
+        if (gi >= M || gj >= N) continue;
+        float v = sC[i][j];
+        if (atomic) {
+            atomicAdd(Cf + (size_t)gi * ldc + gj, v);
+            continue;
+        }
+        if (bias) v += bias[gj];
+        if (relu) v = fmaxf(v, 0.f);
+        if (Cf) Cf[(size_t)gi * ldc + gj] = v;
+        if (Cb) Cb[(size_t)gi * ldc + gj] = __float2bfloat16(v);
+    }
+}
+
+// col[v][t*C + c] = x[z+dz-1][y+dy-1][x+dx-1][c] (0 outside)
+__global__ void im2col_kernel(const __nv_bfloat16* __restrict__ x, __nv_bfloat16* __restrict__ col, int D, int H,
+                              int W, int C) {
+    const long K = 27L * C, total = (long)D * H * W * K;
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const long v = e / K;
+        const int k = (int)(e - v * K), t = k / C, c = k - t * C;
+        const int xx = (int)(v % W), yy = (int)((v / W) % H), zz = (int)(v / ((long)W * H));
+        const int sx = xx + t % 3 - 1, sy = yy + (t / 3) % 3 - 1, sz = zz + t / 9 - 1;
+        __nv_bfloat16 val = __float2bfloat16(0.f);
+        if (sx >= 0 && sx < W && sy >= 0 && sy < H && sz >= 0 && sz < D)
+            val = x[(((long)sz * H + sy) * W + sx) * C + c];
+        col[e] = val;
+    }
+}
+
+// dx[z][y][x][c] = sum over taps t of dcol[v(t)][t*C + c], v(t) = the voxel whose tap t reads (z,y,x)
+__global__ void col2im_kernel(const float* __restrict__ dcol, float* __restrict__ dx, int D, int H, int W, int C) {
+    const long total = (long)D * H * W * C, K = 27L * C;
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const long v = e / C;
+        const int xx = (int)(v % W), yy = (int)((v / W) % H), zz = (int)(v / ((long)W * H));
+        float s = 0.f;
+#pragma unroll
+        for (int t = 0; t < 27; ++t) {
+            // tap t of output voxel o reads o + off(t); so o = (z,y,x) - off(t)
+            const int ox = xx - (t % 3 - 1), oy = yy - ((t / 3) % 3 - 1), oz = zz - (t / 9 - 1);
+            if (ox >= 0 && ox < W && oy >= 0 && oy < H && oz >= 0 && oz < D)
+                s += dcol[(((long)oz * H + oy) * W + ox) * K + (long)t * C + c];
+        }
+        dx[e] = s;
+    }
+}
+
+// Implicit-GEMM forward convolution (Cin a multiple of 8): the A tile (128 voxels x 32
+// channels of one tap) is gathered straight from the channels-last input with 16-byte
+// cp.async copies (zero-filled outside the volume and past Cin), the B tile (BN output
+// channels x the same 32 k) from the weight rows, both double-buffered; no im2col buffer.
+// The accumulators start from the bias; ReLU and the BF16 / FP32 store go through a small
+// per-warp staging tile so that ragged edges are masked.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <int BN>
+__global__ void __launch_bounds__(256) conv_fwd_implicit_kernel(const __nv_bfloat16* __restrict__ x,
+                                                                const __nv_bfloat16* __restrict__ w,
+                                                                const float* __restrict__ bias,
+                                                                __nv_bfloat16* yb, float* yf, int D, int H, int W,
+                                                                int Cin, int Cout, int relu) {
+    constexpr int BM = 128, BK = 32, LDA = BK + 8, LDB = BK + 8, NF = BN / 16;
+    __shared__ __align__(128) __nv_bfloat16 sA[2][BM][LDA];
+    __shared__ __align__(128) __nv_bfloat16 sB[2][BN][LDB];   // [n][k]: matrix_b col-major
+    __shared__ __align__(128) float sBias[16][BN + 4];
+    __shared__ __align__(128) float sStage[8][16][20];
+    const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
+    const long M = (long)D * H * W;
+    const long m0 = (long)blockIdx.x * BM;
+    const int n0 = blockIdx.y * BN;
+    const int K27 = 27 * Cin;
+    for (int e = tid; e < 16 * BN; e += 256) {
+        const int j = e % BN, gj = n0 + j;
+        sBias[e / BN][j] = (bias && gj < Cout) ? bias[gj] : 0.f;
+    }
+    // A: 128 rows x 4 chunks of 8 channels -> 2 chunks per thread; B: BN rows x 4 chunks
+    const int a_row0 = tid >> 2, a_chunk = tid & 3;   // rows a_row0 and a_row0 + 64
+    long av[2];
+    int az[2], ay[2], ax[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        av[h] = m0 + a_row0 + 64 * h;
+        const long v = av[h] < M ? av[h] : 0;
+        ax[h] = (int)(v % W);
+        ay[h] = (int)((v / W) % H);
+        az[h] = (int)(v / ((long)W * H));
+    }
+    const int csteps = (Cin + BK - 1) / BK, nsteps = 27 * csteps;
+    auto load_stage = [&](int step, int buf) {
+        const int tap = step / csteps, c0 = (step - tap * csteps) * BK;
+        const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
+        const int c = c0 + a_chunk * 8;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int sx = ax[h] + dx, sy = ay[h] + dy, sz = az[h] + dz;
+            const bool ok = av[h] < M && c < Cin && sx >= 0 && sx < W && sy >= 0 && sy < H && sz >= 0 && sz < D;
+            const __nv_bfloat16* src = ok ? x + ((((long)sz * H + sy) * W + sx) * Cin + c) : x;
+            cp_async16((uint32_t)__cvta_generic_to_shared(&sA[buf][a_row0 + 64 * h][a_chunk * 8]), src, ok);
+        }
+        for (int e = tid; e < BN * 4; e += 256) {
+            const int j = e >> 2, ch = e & 3, gj = n0 + j, cc = c0 + ch * 8;
+            const bool ok = gj < Cout && cc < Cin;
+            const __nv_bfloat16* src = ok ? w + ((long)gj * K27 + (long)tap * Cin + cc) : w;
+            cp_async16((uint32_t)__cvta_generic_to_shared(&sB[buf][j][ch * 8]), src, ok);
+        }
+        cp_async_commit();
+    };
+    __syncthreads();   // sBias
+    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[NF];
+    const int wm = wid * 16;
+#pragma unroll
+    for (int t = 0; t < NF; ++t) wmma::load_matrix_sync(acc[t], &sBias[0][16 * t], BN + 4, wmma::mem_row_major);
+    load_stage(0, 0);
+    for (int step = 0; step < nsteps; ++step) {
+        const int buf = step & 1;
+        if (step + 1 < nsteps) {
+            load_stage(step + 1, buf ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 16) {
+            wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> fa;
+            wmma::load_matrix_sync(fa, &sA[buf][wm][kk], LDA);
+#pragma unroll
+            for (int t = 0; t < NF; ++t) {
+                wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::col_major> fb;
+                wmma::load_matrix_sync(fb, &sB[buf][16 * t][kk], LDB);
+                wmma::mma_sync(acc[t], fa, fb, acc[t]);
+            }
+        }
+        __syncthreads();   // buffer buf is refilled by the next iteration's load
+    }
+#pragma unroll
+    for (int t = 0; t < NF; ++t) {
+        if (relu) {
+#pragma unroll
+            for (int i = 0; i < acc[t].num_elements; ++i) acc[t].x[i] = fmaxf(acc[t].x[i], 0.f);
+        }
+        wmma::store_matrix_sync(&sStage[wid][0][0], acc[t], 20, wmma::mem_row_major);
+        __syncwarp();
+        for (int e = lane; e < 256; e += 32) {
+            const int i = e >> 4, j = e & 15;
+            const long gi = m0 + wm + i;
+            const int gj = n0 + 16 * t + j;
+            if (gi < M && gj < Cout) {
+                const float v = sStage[wid][i][j];
+                if (yf) yf[gi * Cout + gj] = v;
+                if (yb) yb[gi * Cout + gj] = __float2bfloat16(v);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+int grid_for_conv(long n) { return (int)std::min<long>((n + 255) / 256, 148L * 32); }
+
+}  // namespace
+}  // namespace tigre
+
+using namespace tigre;
+
+extern "C" {
+
+long long tigre_conv3d_col_elems(long D, long H, long W, long C) { return 27LL * D * H * W * C; }
+
+int tigre_conv3d_fwd(const void* d_x, const void* d_w, const float* d_bias, void* d_y_bf16, float* d_y_f32, long D,
+                     long H, long W, long Cin, long Cout, int relu, void* d_col, void* stream) {
+    if (!d_x || !d_w || !d_col || (!d_y_bf16 && !d_y_f32) || D <= 0 || H <= 0 || W <= 0 || Cin <= 0 || Cout <= 0)
+        return fail(TIGRE_ERR_BAD_ASSERT, "bad conv3d arguments");
+    const long M = D * H * W, K = 27 * Cin;
+    if (M * K >= (1L << 31) * 4L || M >= (1L << 31) / 64 * 64) return fail(TIGRE_ERR_BAD_ASSERT, "conv3d too large");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (Cin % 8 == 0 && ((uintptr_t)d_x & 15) == 0 && ((uintptr_t)d_w & 15) == 0) {
+        // implicit GEMM: 16-byte channel chunks need Cin % 8 == 0 and 16-byte aligned bases
+        const int bn = Cout <= 16 ? 16 : (Cout <= 32 ? 32 : 64);
+        dim3 grid((unsigned)((M + 127) / 128), (unsigned)((Cout + bn - 1) / bn), 1);
+        const __nv_bfloat16* xb = (const __nv_bfloat16*)d_x;
+        const __nv_bfloat16* wb = (const __nv_bfloat16*)d_w;
+        if (bn == 16)
+            conv_fwd_implicit_kernel<16><<<grid, 256, 0, st>>>(xb, wb, d_bias, (__nv_bfloat16*)d_y_bf16, d_y_f32,
+                                                              (int)D, (int)H, (int)W, (int)Cin, (int)Cout, relu);
+        else if (bn == 32)
+            conv_fwd_implicit_kernel<32><<<grid, 256, 0, st>>>(xb, wb, d_bias, (__nv_bfloat16*)d_y_bf16, d_y_f32,
+                                                              (int)D, (int)H, (int)W, (int)Cin, (int)Cout, relu);
+        else
+            conv_fwd_implicit_kernel<64><<<grid, 256, 0, st>>>(xb, wb, d_bias, (__nv_bfloat16*)d_y_bf16, d_y_f32,
+                                                              (int)D, (int)H, (int)W, (int)Cin, (int)Cout, relu);
+        TIGRE_LAUNCHED();
+        return TIGRE_SUCCESS;
+    }
+    im2col_kernel<<<grid_for_conv(M * K), 256, 0, st>>>((const __nv_bfloat16*)d_x, (__nv_bfloat16*)d_col, (int)D,
+                                                        (int)H, (int)W, (int)Cin);
+    TIGRE_LAUNCHED();
+    dim3 grid((unsigned)((M + kBM - 1) / kBM), (unsigned)((Cout + kBN - 1) / kBN), 1);
+    gemm_kernel<true, true><<<grid, kThreads, 0, st>>>((const __nv_bfloat16*)d_col, (int)K,
+                                                      (const __nv_bfloat16*)d_w, (int)K, d_y_f32,
+                                                      (__nv_bfloat16*)d_y_bf16, (int)Cout, (int)M, (int)Cout, (int)K,
+                                                      d_bias, relu, (int)K, 0);
+    TIGRE_LAUNCHED();
+    return TIGRE_SUCCESS;
+}
+
+// dx (FP32, channels-last) from dy (BF16, M x Cout) and w; d_dcol: M * 27*Cin floats of scratch.
+int tigre_conv3d_bwd_data(const void* d_dy, const void* d_w, float* d_dx, long D, long H, long W, long Cin, long Cout,
+                          float* d_dcol, void* stream) {
+    if (!d_dy || !d_w || !d_dx || !d_dcol || D <= 0 || H <= 0 || W <= 0 || Cin <= 0 || Cout <= 0)
+        return fail(TIGRE_ERR_BAD_ASSERT, "bad conv3d arguments");
+    const long M = D * H * W, K = 27 * Cin;
+    cudaStream_t st = (cudaStream_t)stream;
+    dim3 grid((unsigned)((M + kBM - 1) / kBM), (unsigned)((K + kBN - 1) / kBN), 1);
+    // dcol (M x K) = dy (M x Cout, row-major) . w (Cout x K, row-major)
+    gemm_kernel<true, false><<<grid, kThreads, 0, st>>>((const __nv_bfloat16*)d_dy, (int)Cout,
+                                                       (const __nv_bfloat16*)d_w, (int)K, d_dcol, nullptr, (int)K,
+                                                       (int)M, (int)K, (int)Cout, nullptr, 0, (int)Cout, 0);
+    TIGRE_LAUNCHED();
+    col2im_kernel<<<grid_for_conv(M * Cin), 256, 0, st>>>(d_dcol, d_dx, (int)D, (int)H, (int)W, (int)Cin);
+    TIGRE_LAUNCHED();
+    return TIGRE_SUCCESS;
+}
+
+// dw (FP32, Cout x 27*Cin) += dy^T . col, with col = im2col(x) recomputed into d_col.
+int tigre_conv3d_bwd_weight(const void* d_x, const void* d_dy, float* d_dw, long D, long H, long W, long Cin,
+                            long Cout, void* d_col, void* stream) {
+    if (!d_x || !d_dy || !d_dw || !d_col || D <= 0 || H <= 0 || W <= 0 || Cin <= 0 || Cout <= 0)
+        return fail(TIGRE_ERR_BAD_ASSERT, "bad conv3d arguments");
+    const long M = D * H * W, K = 27 * Cin;
+    cudaStream_t st = (cudaStream_t)stream;
+    im2col_kernel<<<grid_for_conv(M * K), 256, 0, st>>>((const __nv_bfloat16*)d_x, (__nv_bfloat16*)d_col, (int)D,
+                                                        (int)H, (int)W, (int)Cin);
+    TIGRE_LAUNCHED();
+    // the reduction runs over the M voxels: split it over blocks, FP32 atomics into dw
+    const int chunk = 4096;
+    dim3 grid((unsigned)((Cout + kBM - 1) / kBM), (unsigned)((K + kBN - 1) / kBN), (unsigned)((M + chunk - 1) / chunk));
+    // op(A) = dy^T (Cout x M): stored M x Cout row-major -> element (i=co, k=v) at dy[v * Cout + co]
+    gemm_kernel<false, false><<<grid, kThreads, 0, st>>>((const __nv_bfloat16*)d_dy, (int)Cout,
+                                                        (const __nv_bfloat16*)d_col, (int)K, d_dw, nullptr, (int)K,
+                                                        (int)Cout, (int)K, (int)M, nullptr, 0, chunk, 1);
+    TIGRE_LAUNCHED();
+    return TIGRE_SUCCESS;
+}
+
+}  // extern "C"
