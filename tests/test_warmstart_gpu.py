@@ -20,8 +20,12 @@ def _ref_weights(w, cin, cout):
 
 
 @pytest.mark.parametrize("shape,cin,cout", [((6, 5, 7), 3, 5), ((20, 16, 16), 40, 70), ((8, 8, 8), 1, 16),
-                                            ((4, 9, 6), 48, 1)])
-def test_conv3d_matches_torch_fp32(shape, cin, cout):
+                                            ((4, 9, 6), 48, 1),
+                                            # tcgen05 path: Cin % 8 == 0 and Cout % 16 == 0, N tiles 16..128
+                                            ((8, 6, 10), 16, 16), ((7, 9, 11), 8, 32), ((9, 8, 7), 48, 48),
+                                            ((6, 6, 6), 24, 64), ((5, 7, 9), 16, 128), ((3, 4, 5), 64, 192)])
+@pytest.mark.parametrize("tcgen05", [0, 1])
+def test_conv3d_matches_torch_fp32(shape, cin, cout, tcgen05):
     import torch
     import torch.nn.functional as F
     from tigre_b200 import _native as N
@@ -51,7 +55,11 @@ def test_conv3d_matches_torch_fp32(shape, cin, cout):
     dx = torch.empty((D, H, W, cin), dtype=torch.float32, device="cuda")
     dw = torch.zeros((cout, 27 * cin), dtype=torch.float32, device="cuda")
     p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
-    N.check(L.tigre_conv3d_fwd(p(xd), p(wd), p(bd), None, p(y), D, H, W, cin, cout, 0, p(col), None), "fwd")
+    old = L.tigre_conv3d_set_tcgen05(tcgen05)
+    try:
+        N.check(L.tigre_conv3d_fwd(p(xd), p(wd), p(bd), None, p(y), D, H, W, cin, cout, 0, p(col), None), "fwd")
+    finally:
+        L.tigre_conv3d_set_tcgen05(old)
     N.check(L.tigre_conv3d_bwd_data(p(dyd), p(wd), p(dx), D, H, W, cin, cout, p(dcol), None), "data")
     N.check(L.tigre_conv3d_bwd_weight(p(xd), p(dyd), p(dw), D, H, W, cin, cout, p(col), None), "weight")
     torch.cuda.synchronize()

@@ -16,6 +16,8 @@
 #include <cuda_bf16.h>
 #include <mma.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cstdint>
 
 #include "tigre_internal.h"
@@ -249,6 +251,223 @@ __global__ void __launch_bounds__(256) conv_fwd_implicit_kernel(const __nv_bfloa
     }
 }
 
+// ---- tcgen05 implicit-GEMM forward convolution (Cin % 8 == 0, Cout % 16 == 0) ----
+//
+// One CTA of 4 warps computes a 128-voxel x BN-channel tile.  Per K step (one tap x 32 input
+// channels) all threads gather the A tile (128 x 32 BF16) and the B tile (BN x 32) with 16-byte
+// cp.async copies into the K-major, unswizzled canonical layout of the tensor-core operands
+// (8-row x 16-byte core matrices; LBO = 128 B between the four core matrices along K, SBO =
+// 512 B between 8-row groups), then one thread issues two tcgen05.mma (K = 16 each) that
+// accumulate in TMEM (128 lanes x BN FP32 columns) and commits them to the stage's mbarrier.
+// Two smem stages: a stage is refilled only after the MMAs that read it have completed (their
+// mbarrier phase).  The epilogue reads TMEM with tcgen05.ld (warp w: lanes 32w..32w+31 = its
+// 32 voxels), adds the bias, applies ReLU and stores.  Every mbarrier wait is bounded; on
+// expiry the tile is left unwritten and the status word gets bit 0.
+constexpr unsigned kTcWaitLimit = 1u << 20;   // polls of ~100 ns: about 0.1 s
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+           (1ull << 46);   // descriptor version 1; base offset 0; no swizzle
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t phase) {
+    for (unsigned i = 0; i < kTcWaitLimit; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        if (ok) return true;
+        __nanosleep(64);
+    }
+    return false;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128) conv_fwd_tc_kernel(const __nv_bfloat16* __restrict__ x,
+                                                          const __nv_bfloat16* __restrict__ w,
+                                                          const float* __restrict__ bias, __nv_bfloat16* yb,
+                                                          float* yf, int D, int H, int W, int Cin, int Cout, int relu,
+                                                          int* status) {
+    static_assert(BN % 16 == 0 && BN >= 16 && BN <= 128, "N tile");
+    constexpr int BM = 128, BK = 64, STAGES = 3;
+    constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
+    constexpr uint32_t TCOLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : 128);
+    constexpr uint32_t LBO = 128, SBO = 1024;   // K-adjacent core matrices / 8-row groups
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __shared__ __align__(8) unsigned long long mma_bar[STAGES];
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31;
+    const uint32_t base = ((uint32_t)__cvta_generic_to_shared(tc_smem) + 1023u) & ~1023u;
+    const long M = (long)D * H * W;
+    const long m0 = (long)blockIdx.x * BM;
+    const int n0 = blockIdx.y * BN;
+    const int K27 = 27 * Cin;
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(&mma_bar[s]))
+                         : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (wid == 0) {
+        const uint32_t slot = (uint32_t)__cvta_generic_to_shared(&tmem_slot);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    // A loads: eight lanes take one voxel's eight consecutive 16-byte chunks (128 contiguous bytes
+    // when the chunks stay in one tap), so a warp reads 4 voxels per copy; this thread serves rows
+    // (tid >> 3) + 16 i, i = 0..7, always chunk tid & 7
+    const int jA = tid & 7;
+    int rx[8], ry[8], rz[8];
+    bool rin[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const long av = m0 + (tid >> 3) + 16 * i;
+        rin[i] = av < M;
+        const long vv = rin[i] ? av : 0;
+        rx[i] = (int)(vv % W);
+        ry[i] = (int)((vv / W) % H);
+        rz[i] = (int)(vv / ((long)W * H));
+    }
+    const int nsteps = (K27 + BK - 1) / BK;
+    auto tile_off = [](int r, int j) -> uint32_t { return (uint32_t)((r >> 3) * SBO + j * LBO + (r & 7) * 16); };
+    // a step covers K range [64 step, 64 step + 64) of the flattened (tap, channel) index, eight
+    // 16-byte chunks per row; a chunk never straddles two taps (Cin % 8 == 0)
+    auto load_stage = [&](int step, int s) {
+        const uint32_t sa = base + (uint32_t)s * STAGE_BYTES, sb = sa + A_BYTES;
+        const int k = step * BK + 8 * jA;
+        const int tap = k / Cin, c = k - tap * Cin;
+        const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int sx = rx[i] + dx, sy = ry[i] + dy, sz = rz[i] + dz;
+            const bool ok = k < K27 && rin[i] && sx >= 0 && sx < W && sy >= 0 && sy < H && sz >= 0 && sz < D;
+            const long off = (((long)sz * H + sy) * W + sx) * Cin + c;
+            cp_async16(sa + tile_off((tid >> 3) + 16 * i, jA), ok ? (const void*)(x + off) : (const void*)x, ok);
+        }
+        for (int e = tid; e < BN * 8; e += 128) {
+            const int r = e >> 3, j = e & 7, gj = n0 + r, k = step * BK + 8 * j;
+            const bool ok = gj < Cout && k < K27;
+            cp_async16(sb + tile_off(r, j), ok ? (const void*)(w + (long)gj * K27 + k) : (const void*)w, ok);
+        }
+    };
+    constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(BM >> 4) << 24);
+    bool ok_all = true;
+    uint32_t phase_bits = 0u;   // bit s: parity to wait for on stage s
+    unsigned issued_bits = 0u;
+    auto wait_stage = [&](int s) {
+        if ((issued_bits >> s) & 1u) {
+            const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&mma_bar[s]);
+            if (ok_all && !tc_wait(bar, (phase_bits >> s) & 1u)) ok_all = false;
+            phase_bits ^= 1u << s;
+            issued_bits &= ~(1u << s);
+        }
+    };
+    // prologue: the first STAGES-1 steps in flight (one cp.async group each, empty ones too)
+    for (int p = 0; p < STAGES - 1; ++p) {
+        if (p < nsteps) load_stage(p, p);
+        cp_async_commit();
+    }
+    for (int step = 0; step < nsteps; ++step) {
+        const int s = step % STAGES;
+        cp_async_wait<STAGES - 2>();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0 && ok_all) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = base + (uint32_t)s * STAGE_BYTES, sb = sa + A_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk) {
+                const uint64_t da = smem_desc(sa + 2u * LBO * kk, LBO, SBO);
+                const uint64_t db = smem_desc(sb + 2u * LBO * kk, LBO, SBO);
+                const uint32_t acc = (step > 0 || kk > 0) ? 1u : 0u;
+                const uint32_t no_mask = 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(no_mask)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             (uint32_t)__cvta_generic_to_shared(&mma_bar[s]))
+                         : "memory");
+        }
+        issued_bits |= 1u << s;
+        // refill the stage of step-1 with step+STAGES-1 once the MMAs of step-1 have read it
+        const int next = step + STAGES - 1;
+        const int ns = next % STAGES;
+        if (next < nsteps) {
+            wait_stage(ns);
+            load_stage(next, ns);
+        }
+        cp_async_commit();
+    }
+    for (int s = 0; s < STAGES; ++s) wait_stage(s);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const long row = m0 + 32 * wid + lane;
+    if (ok_all) {
+#pragma unroll
+        for (int t = 0; t < BN / 16; ++t) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + ((uint32_t)(32 * wid) << 16) + (uint32_t)(16 * t);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < M) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int gj = n0 + 16 * t + j;
+                    if (gj < Cout) {
+                        float v = __uint_as_float(r[j]) + (bias ? bias[gj] : 0.f);
+                        if (relu) v = fmaxf(v, 0.f);
+                        if (yf) yf[row * Cout + gj] = v;
+                        if (yb) yb[row * Cout + gj] = __float2bfloat16(v);
+                    }
+                }
+            }
+        }
+    } else if (tid == 0 && status) {
+        atomicOr(status, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (wid == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS) : "memory");
+    }
+}
+
+// Launch of the tcgen05 kernel with dynamic shared memory sized so that at most 512 / TCOLS CTAs
+// share an SM: their TMEM allocations then always fit the SM's 512 columns.
+template <int BN>
+int launch_conv_tc(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias, __nv_bfloat16* yb, float* yf,
+                   int D, int H, int W, int Cin, int Cout, int relu, int* status, cudaStream_t st) {
+    constexpr int TCOLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : 128);
+    constexpr int max_ctas = 512 / TCOLS;
+    const long M = (long)D * H * W;
+    const int need = 1024 + 3 * (128 * 64 * 2 + BN * 64 * 2);
+    const int floor_smem = max_ctas >= 16 ? 0 : 233472 / (max_ctas + 1) - 1024 + 64;
+    const int smem = std::max(need, floor_smem);
+    TIGRE_CUDA(cudaFuncSetAttribute(conv_fwd_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    dim3 grid((unsigned)((M + 127) / 128), (unsigned)(Cout / BN), 1);
+    conv_fwd_tc_kernel<BN><<<grid, 128, smem, st>>>(x, w, bias, yb, yf, D, H, W, Cin, Cout, relu, status);
+    TIGRE_LAUNCHED();
+    return TIGRE_SUCCESS;
+}
+
 int grid_for_conv(long n) { return (int)std::min<long>((n + 255) / 256, 148L * 32); }
 
 }  // namespace
@@ -256,7 +475,14 @@ int grid_for_conv(long n) { return (int)std::min<long>((n + 255) / 256, 148L * 3
 
 using namespace tigre;
 
+// Forward path selection: the warp-level implicit GEMM is the default (faster at every U-Net
+// shape but 128^3 16->16 on B200: its 8 warps keep more gathers in flight than the tcgen05 kernel,
+// whose loads for a step wait for the MMAs two steps back); the tcgen05 kernel is opt-in.
+static std::atomic<int> g_conv_tcgen05{0};
+
 extern "C" {
+
+int tigre_conv3d_set_tcgen05(int on) { return g_conv_tcgen05.exchange(on ? 1 : 0); }
 
 long long tigre_conv3d_col_elems(long D, long H, long W, long C) { return 27LL * D * H * W * C; }
 
@@ -267,6 +493,19 @@ int tigre_conv3d_fwd(const void* d_x, const void* d_w, const float* d_bias, void
     const long M = D * H * W, K = 27 * Cin;
     if (M * K >= (1L << 31) * 4L || M >= (1L << 31) / 64 * 64) return fail(TIGRE_ERR_BAD_ASSERT, "conv3d too large");
     cudaStream_t st = (cudaStream_t)stream;
+    if (g_conv_tcgen05.load() && Cin % 8 == 0 && Cout % 16 == 0 && ((uintptr_t)d_x & 15) == 0 &&
+        ((uintptr_t)d_w & 15) == 0) {
+        // tensor-core (tcgen05) implicit GEMM: N tile = the largest of 128 / 64 / 48 / 32 / 16 dividing Cout
+        const __nv_bfloat16* xb = (const __nv_bfloat16*)d_x;
+        const __nv_bfloat16* wb = (const __nv_bfloat16*)d_w;
+        __nv_bfloat16* yb = (__nv_bfloat16*)d_y_bf16;
+        const int iD = (int)D, iH = (int)H, iW = (int)W, ci = (int)Cin, co = (int)Cout;
+        if (Cout % 128 == 0) return launch_conv_tc<128>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, nullptr, st);
+        if (Cout % 64 == 0) return launch_conv_tc<64>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, nullptr, st);
+        if (Cout % 48 == 0) return launch_conv_tc<48>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, nullptr, st);
+        if (Cout % 32 == 0) return launch_conv_tc<32>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, nullptr, st);
+        return launch_conv_tc<16>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, nullptr, st);
+    }
     if (Cin % 8 == 0 && ((uintptr_t)d_x & 15) == 0 && ((uintptr_t)d_w & 15) == 0) {
         // implicit GEMM: 16-byte channel chunks need Cin % 8 == 0 and 16-byte aligned bases
         const int bn = Cout <= 16 ? 16 : (Cout <= 32 ? 32 : 64);
