@@ -428,15 +428,29 @@ __global__ void __launch_bounds__(128) conv_fwd_tc_kernel(const __nv_bfloat16* _
                 : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (row < M) {
+                // this thread's 16 consecutive channels: 16-byte vector stores (Cout % BN == 0, so
+                // every column exists and the row segment is 32-byte aligned)
+                float v[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    const int gj = n0 + 16 * t + j;
-                    if (gj < Cout) {
-                        float v = __uint_as_float(r[j]) + (bias ? bias[gj] : 0.f);
-                        if (relu) v = fmaxf(v, 0.f);
-                        if (yf) yf[row * Cout + gj] = v;
-                        if (yb) yb[row * Cout + gj] = __float2bfloat16(v);
+                    v[j] = __uint_as_float(r[j]) + (bias ? bias[n0 + 16 * t + j] : 0.f);
+                    if (relu) v[j] = fmaxf(v[j], 0.f);
+                }
+                const long o = row * Cout + n0 + 16 * t;
+                if (yf) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        reinterpret_cast<float4*>(yf + o)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                }
+                if (yb) {
+                    uint32_t pk[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+                        pk[q] = *reinterpret_cast<const uint32_t*>(&h);
                     }
+                    reinterpret_cast<uint4*>(yb + o)[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                    reinterpret_cast<uint4*>(yb + o)[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
                 }
             }
         }
@@ -475,14 +489,16 @@ int grid_for_conv(long n) { return (int)std::min<long>((n + 255) / 256, 148L * 3
 
 using namespace tigre;
 
-// Forward path selection: the warp-level implicit GEMM is the default (faster at every U-Net
-// shape but 128^3 16->16 on B200: its 8 warps keep more gathers in flight than the tcgen05 kernel,
-// whose loads for a step wait for the MMAs two steps back); the tcgen05 kernel is opt-in.
-static std::atomic<int> g_conv_tcgen05{0};
+// Forward path selection (when Cin % 8 == 0 and Cout % 16 == 0): 0 = warp-level implicit GEMM,
+// 1 = tcgen05 implicit GEMM, 2 (default) = tcgen05 for narrow layers (Cin <= 16 or Cout == 16),
+// where it is faster on B200, and the warp-level kernel for the wider ones, where its 8 warps keep
+// more gathers in flight than the tcgen05 kernel, whose loads for a step wait for the MMAs two
+// steps back (measured per shape, 16^3 to 128^3).
+static std::atomic<int> g_conv_tcgen05{2};
 
 extern "C" {
 
-int tigre_conv3d_set_tcgen05(int on) { return g_conv_tcgen05.exchange(on ? 1 : 0); }
+int tigre_conv3d_set_tcgen05(int mode) { return g_conv_tcgen05.exchange(mode < 0 || mode > 2 ? 2 : mode); }
 
 long long tigre_conv3d_col_elems(long D, long H, long W, long C) { return 27LL * D * H * W * C; }
 
@@ -493,8 +509,9 @@ int tigre_conv3d_fwd(const void* d_x, const void* d_w, const float* d_bias, void
     const long M = D * H * W, K = 27 * Cin;
     if (M * K >= (1L << 31) * 4L || M >= (1L << 31) / 64 * 64) return fail(TIGRE_ERR_BAD_ASSERT, "conv3d too large");
     cudaStream_t st = (cudaStream_t)stream;
-    if (g_conv_tcgen05.load() && Cin % 8 == 0 && Cout % 16 == 0 && ((uintptr_t)d_x & 15) == 0 &&
-        ((uintptr_t)d_w & 15) == 0) {
+    const int tc_mode = g_conv_tcgen05.load();
+    const bool tc_wanted = tc_mode == 1 || (tc_mode == 2 && (Cin <= 16 || Cout == 16));
+    if (tc_wanted && Cin % 8 == 0 && Cout % 16 == 0 && ((uintptr_t)d_x & 15) == 0 && ((uintptr_t)d_w & 15) == 0) {
         // tensor-core (tcgen05) implicit GEMM: N tile = the largest of 128 / 64 / 48 / 32 / 16 dividing Cout
         const __nv_bfloat16* xb = (const __nv_bfloat16*)d_x;
         const __nv_bfloat16* wb = (const __nv_bfloat16*)d_w;
