@@ -64,6 +64,14 @@ int tigre_ax(TigrePlan* plan, const void* d_vol, int vdt, void* d_proj, int pdt,
     if (projector == TIGRE_PROJ_SIDDON && plan->columns) {
         // z-fast working copy; the cell-interval kernel needs deeper zero pads
         const int zpad = plan->cells_zpad > 0 ? plan->cells_zpad : 1;
+        if (plan->cells_zpad > 0 && vdt != TIGRE_F32) {
+            // 16-bit storage: the working copy is built in FP32 (exact), so the cell kernel runs
+            // its FP32 form and gives the same sums as on a widened volume
+            float* sf = (float*)plan_scratch(plan, (size_t)d.nX * d.nY * (d.nZ + 2 * zpad) * sizeof(float), st, &rc);
+            if (rc) return rc;
+            if ((rc = launch_make_zfast_f32(d_vol, vdt, sf, d.nX, d.nY, d.nZ, zpad, st))) return rc;
+            return launch_siddon_cells(plan, sf, TIGRE_F32, d_proj, pdt, a0, a1, st);
+        }
         void* s = plan_scratch(plan, (size_t)d.nX * d.nY * (d.nZ + 2 * zpad) * es, st, &rc);
         if (rc) return rc;
         if ((rc = launch_make_zfast(d_vol, vdt, s, d.nX, d.nY, d.nZ, zpad, st))) return rc;
@@ -87,6 +95,21 @@ int tigre_ax(TigrePlan* plan, const void* d_vol, int vdt, void* d_proj, int pdt,
         // (offsets rounded to 256 bytes: the quads are read as 8- or 16-byte vectors)
         const size_t padded = ((size_t)(d.nX + 3) * (d.nY + 3) * (d.nZ + 3) * es + 255) / 256 * 256;
         const bool nearest = d.accuracy > 1.0;
+        if (!nearest && vdt != TIGRE_F32) {
+            // 16-bit storage: FP32 corner quads (exact widening) for the FP32 sampling kernel
+            const size_t pf = ((size_t)(d.nX + 3) * (d.nY + 3) * (d.nZ + 3) * sizeof(float) + 255) / 256 * 256;
+            char* s = (char*)plan_scratch(plan, padded + 8 * pf, st, &rc);
+            if (rc) return rc;
+            void* vx = s;
+            float* qx = (float*)(s + padded);
+            float* qy = (float*)(s + padded + 4 * pf);
+            for (int l = 0; l < 2; ++l) {
+                if (!(l ? l1 : l0)) continue;
+                if ((rc = launch_make_layout(d_vol, vdt, vx, d.nX, d.nY, d.nZ, l, 1, 2, st))) return rc;
+                if ((rc = launch_make_quads_f32(vx, vdt, l ? qy : qx, d.nX, d.nY, d.nZ, l, st))) return rc;
+            }
+            return launch_interp(plan, nullptr, nullptr, qx, qy, TIGRE_F32, d_proj, pdt, a0, a1, st);
+        }
         char* s = (char*)plan_scratch(plan, padded * (nearest ? 2 : 9), st, &rc);
         if (rc) return rc;
         void* vx = s;
@@ -128,6 +151,15 @@ int tigre_atb_ex(TigrePlan* plan, const void* d_proj, int pdt, void* d_vol, int 
     const Dims& d = plan->d;
     const int na = a1 - a0;
     int rc = TIGRE_SUCCESS;
+    if (pdt != TIGRE_F32 && (vdt == TIGRE_F32 || vdt == TIGRE_BF16) && bp_tma_supported(plan, TIGRE_F32)) {
+        // 16-bit projections: widened to FP32 (exact) into a pitched copy, then the FP32 patches
+        const int pitch = (d.nU + 3) / 4 * 4;
+        float* s = (float*)plan_scratch(plan, (size_t)na * d.nV * pitch * sizeof(float), st, &rc);
+        if (rc) return rc;
+        if ((rc = launch_repitch_projections_f32(d_proj, pdt, s, na, d.nV, d.nU, pitch, st))) return rc;
+        return launch_backproject_tma(plan, s, pitch, TIGRE_F32, d_vol, vdt, backprojector == TIGRE_BACKPROJ_MATCHED,
+                                      a0, a1, accumulate, st);
+    }
     if (bp_tma_supported(plan, pdt)) {
         const int align = 16 / (int)dtype_size(pdt);
         if (d.nU % align == 0 && ((uintptr_t)d_proj % 16) == 0)

@@ -239,6 +239,8 @@ int launch_interp(TigrePlan* P, const void* vol_x, const void* vol_y, const void
         else if (vdt == TIGRE_F16 && pdt == TIGRE_F16) launch_typed<__half, __half>(ac, nearest, grid, block, st);
         else if (vdt == TIGRE_BF16 && pdt == TIGRE_F32) launch_typed<__nv_bfloat16, float>(ac, nearest, grid, block, st);
         else if (vdt == TIGRE_F16 && pdt == TIGRE_F32) launch_typed<__half, float>(ac, nearest, grid, block, st);
+        else if (vdt == TIGRE_F32 && pdt == TIGRE_BF16) launch_typed<float, __nv_bfloat16>(ac, nearest, grid, block, st);
+        else if (vdt == TIGRE_F32 && pdt == TIGRE_F16) launch_typed<float, __half>(ac, nearest, grid, block, st);
         else return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype pair for interpolated projection");
         TIGRE_LAUNCHED();
     }

@@ -55,15 +55,15 @@ __global__ void make_layout_kernel(const T* __restrict__ src, T* __restrict__ ds
 // z-fastest copy with P zero slices before and after each z-run: dst (X, Y, Z+2P),
 // dst[(x*Y + y)*(Z+2P) + zp] = src(z = zp-P, y, x), zero where zp-P is outside [0, Z).
 // One y per block row of the grid; a 32x32 (zp, x) tile goes through shared memory.
-template <typename T>
-__global__ void make_zfast_kernel(const T* __restrict__ src, T* __restrict__ dst, int nX, int nY, int nZ, int P) {
+template <typename Ts, typename T>
+__global__ void make_zfast_kernel(const Ts* __restrict__ src, T* __restrict__ dst, int nX, int nY, int nZ, int P) {
     __shared__ T tile[TILE][TILE + 1];
     const int ZP = nZ + 2 * P;
     const int zp0 = blockIdx.x * TILE, x0 = blockIdx.y * TILE, y = blockIdx.z;
     for (int j = threadIdx.y; j < TILE; j += blockDim.y) {
         const int zp = zp0 + j, x = x0 + threadIdx.x, z = zp - P;
         T v = from_f32<T>(0.f);
-        if (z >= 0 && z < nZ && x < nX) v = src[((size_t)z * nY + y) * nX + x];
+        if (z >= 0 && z < nZ && x < nX) v = from_f32<T>(to_f32<Ts>(src[((size_t)z * nY + y) * nX + x]));
         tile[j][threadIdx.x] = v;
     }
     __syncthreads();
@@ -81,18 +81,19 @@ __global__ void make_zfast_kernel(const T* __restrict__ src, T* __restrict__ dst
 template <typename T>
 struct Quad4 { T v[4]; };
 
-template <typename T>
-__global__ void make_quads_kernel(const T* __restrict__ pad, Quad4<T>* __restrict__ dst, int F, int O, int Z) {
+template <typename Ts, typename T>
+__global__ void make_quads_kernel(const Ts* __restrict__ pad, Quad4<T>* __restrict__ dst, int F, int O, int Z) {
     const long plane = (long)F * O, total = plane * Z;
+    auto cv = [](Ts v) { return from_f32<T>(to_f32<Ts>(v)); };
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const int f = (int)(i % F);
         const long zp = i / plane;
         const bool f1 = f + 1 < F, z1 = zp + 1 < Z;
         Quad4<T> q;
-        q.v[0] = pad[i];
-        q.v[1] = f1 ? pad[i + 1] : from_f32<T>(0.f);
-        q.v[2] = z1 ? pad[i + plane] : from_f32<T>(0.f);
-        q.v[3] = (f1 && z1) ? pad[i + plane + 1] : from_f32<T>(0.f);
+        q.v[0] = cv(pad[i]);
+        q.v[1] = f1 ? cv(pad[i + 1]) : from_f32<T>(0.f);
+        q.v[2] = z1 ? cv(pad[i + plane]) : from_f32<T>(0.f);
+        q.v[3] = (f1 && z1) ? cv(pad[i + plane + 1]) : from_f32<T>(0.f);
         dst[i] = q;
     }
 }
@@ -111,13 +112,13 @@ __global__ void pad_projections_kernel(const T* __restrict__ src, T* __restrict_
     }
 }
 
-template <typename T>
-__global__ void repitch_kernel(const T* __restrict__ src, T* __restrict__ dst, int nU, int pitch, long rows) {
+template <typename Ts, typename T>
+__global__ void repitch_kernel(const Ts* __restrict__ src, T* __restrict__ dst, int nU, int pitch, long rows) {
     const long total = rows * pitch;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const long r = i / pitch;
         const int c = (int)(i - r * pitch);
-        dst[i] = c < nU ? src[r * nU + c] : from_f32<T>(0.f);
+        dst[i] = c < nU ? from_f32<T>(to_f32<Ts>(src[r * nU + c])) : from_f32<T>(0.f);
     }
 }
 
@@ -128,7 +129,18 @@ int launch_repitch_projections(const void* src, int dtype, void* dst, int nA, in
     const long rows = (long)nA * nV;
     const long want = (rows * pitch + 255) / 256;
     const int grid = (int)std::min<long>(want, 148L * 32);
-    TIGRE_DISPATCH_DTYPE(dtype, T, { repitch_kernel<T><<<grid, 256, 0, st>>>((const T*)src, (T*)dst, nU, pitch, rows); });
+    TIGRE_DISPATCH_DTYPE(dtype, T, { repitch_kernel<T, T><<<grid, 256, 0, st>>>((const T*)src, (T*)dst, nU, pitch, rows); });
+    TIGRE_LAUNCHED();
+    return TIGRE_SUCCESS;
+}
+
+// 16-bit projections widened to FP32 on the way (exact), same pitching as above
+int launch_repitch_projections_f32(const void* src, int dtype, float* dst, int nA, int nV, int nU, int pitch,
+                                   cudaStream_t st) {
+    const long rows = (long)nA * nV;
+    const long want = (rows * pitch + 255) / 256;
+    const int grid = (int)std::min<long>(want, 148L * 32);
+    TIGRE_DISPATCH_DTYPE(dtype, T, { repitch_kernel<T, float><<<grid, 256, 0, st>>>((const T*)src, dst, nU, pitch, rows); });
     TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
@@ -152,7 +164,18 @@ int launch_make_zfast(const void* src, int dtype, void* dst, int nX, int nY, int
     dim3 block(TILE, 8);
     dim3 grid((nZ + 2 * zpad + TILE - 1) / TILE, (nX + TILE - 1) / TILE, nY);
     TIGRE_DISPATCH_DTYPE(dtype, T, {
-        make_zfast_kernel<T><<<grid, block, 0, st>>>((const T*)src, (T*)dst, nX, nY, nZ, zpad);
+        make_zfast_kernel<T, T><<<grid, block, 0, st>>>((const T*)src, (T*)dst, nX, nY, nZ, zpad);
+    });
+    TIGRE_LAUNCHED();
+    return TIGRE_SUCCESS;
+}
+
+// FP32 z-fast copy of a volume of any storage type (16-bit values widen exactly)
+int launch_make_zfast_f32(const void* src, int dtype, float* dst, int nX, int nY, int nZ, int zpad, cudaStream_t st) {
+    dim3 block(TILE, 8);
+    dim3 grid((nZ + 2 * zpad + TILE - 1) / TILE, (nX + TILE - 1) / TILE, nY);
+    TIGRE_DISPATCH_DTYPE(dtype, T, {
+        make_zfast_kernel<T, float><<<grid, block, 0, st>>>((const T*)src, dst, nX, nY, nZ, zpad);
     });
     TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
@@ -163,7 +186,19 @@ int launch_make_quads(const void* pad, int dtype, void* dst, int nX, int nY, int
     const long total = (long)F * O * Z;
     const int grid = (int)std::min<long>((total + 255) / 256, 148L * 32);
     TIGRE_DISPATCH_DTYPE(dtype, T, {
-        make_quads_kernel<T><<<grid, 256, 0, st>>>((const T*)pad, (Quad4<T>*)dst, F, O, Z);
+        make_quads_kernel<T, T><<<grid, 256, 0, st>>>((const T*)pad, (Quad4<T>*)dst, F, O, Z);
+    });
+    TIGRE_LAUNCHED();
+    return TIGRE_SUCCESS;
+}
+
+// FP32 corner quads from a padded copy of any storage type
+int launch_make_quads_f32(const void* pad, int dtype, float* dst, int nX, int nY, int nZ, int layout, cudaStream_t st) {
+    const int F = (layout ? nY : nX) + 3, O = (layout ? nX : nY) + 3, Z = nZ + 3;
+    const long total = (long)F * O * Z;
+    const int grid = (int)std::min<long>((total + 255) / 256, 148L * 32);
+    TIGRE_DISPATCH_DTYPE(dtype, T, {
+        make_quads_kernel<T, float><<<grid, 256, 0, st>>>((const T*)pad, (Quad4<float>*)dst, F, O, Z);
     });
     TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;

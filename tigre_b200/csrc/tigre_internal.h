@@ -147,6 +147,10 @@ int launch_make_layout(const void* src, int dtype, void* dst, int nX, int nY, in
 int launch_pad_projections(const void* src, int dtype, void* dst, int nA, int nV, int nU, cudaStream_t st);
 int launch_make_quads(const void* pad, int dtype, void* dst, int nX, int nY, int nZ, int layout, cudaStream_t st);
 int launch_make_zfast(const void* src, int dtype, void* dst, int nX, int nY, int nZ, int zpad, cudaStream_t st);
+int launch_make_zfast_f32(const void* src, int dtype, float* dst, int nX, int nY, int nZ, int zpad, cudaStream_t st);
+int launch_make_quads_f32(const void* pad, int dtype, float* dst, int nX, int nY, int nZ, int layout, cudaStream_t st);
+int launch_repitch_projections_f32(const void* src, int dtype, float* dst, int nA, int nV, int nU, int pitch,
+                                   cudaStream_t st);
 
 int launch_siddon(TigrePlan* p, const void* vol_x, const void* vol_y, int vdt, void* proj, int pdt, int a0, int a1,
                   cudaStream_t st);
