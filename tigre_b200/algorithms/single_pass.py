@@ -13,7 +13,6 @@ import copy
 
 import numpy as np
 
-from .. import _native as N
 from .. import projectors as P
 from ..utilities import filtering as F
 from ._common import Problem, torch
