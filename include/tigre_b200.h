@@ -47,6 +47,10 @@ extern "C" {
 #define TIGRE_BACKPROJ_FDK 0
 #define TIGRE_BACKPROJ_MATCHED 1
 
+/* Rounding of FP32 results into 16-bit storage (tigre_sart_update). */
+#define TIGRE_ROUND_NEAREST 0
+#define TIGRE_ROUND_STOCHASTIC 1
+
 /*
  * Per-call geometry: field-for-field the layout of `struct Geometry`
  * (Common/CUDA/types_TIGRE.hpp:48-85).  Per-angle arrays have nangles entries.
@@ -232,6 +236,17 @@ int tigre_tv_denoise(const float* d_src, float* d_dst, long nx, long ny, long nz
 int tigre_tv_gradient(const void* d_img, int dtype, float* d_grad, long nx, long ny, long nz, void* stream);
 /* TV value sum_i |grad f_i| consistent with tigre_tv_gradient; added into *d_out (FP64). */
 int tigre_tv_value(const void* d_img, int dtype, long nx, long ny, long nz, double* d_out, void* stream);
+
+/* SART-family volume update in place: d_x[z][j] <- max(d_x + (lambda / d_v[j]) * d_bp[z][j], 0)
+ * for z < nz, j < nyx (the clip only when noneg), the update of IterativeReconAlg.update_image
+ * (Python/tigre/algorithms/iterative_recon_alg.py:389-401) with the clip of art_data_minimizing
+ * (:344-345) in one pass.  d_x: storage dtype; d_bp: FP32 backprojection; d_v: FP32 plane of nyx
+ * weights.  FP32 arithmetic in the reference's operation order.  rounding: TIGRE_ROUND_NEAREST, or
+ * TIGRE_ROUND_STOCHASTIC for 16-bit storage (Philox4x32-10 bits from (seed, step, voxel); FP32
+ * storage ignores it). */
+int tigre_sart_update(void* d_x, int dtype, const float* d_bp, const float* d_v, float lambda, int noneg,
+                      long long nz, long long nyx, int rounding, unsigned long long seed, unsigned long long step,
+                      void* stream);
 
 /* Device noise (same generator as tigre_noise_1d); d_in and d_out may alias. */
 int tigre_add_noise(const float* d_in, float* d_out, long long n, int gaussian, float mu, float sigma,

@@ -358,6 +358,63 @@ def mlem(proj, geo, angles, niter, x0=None):
     return x.astype(np.float32)
 
 
+def ossart(proj, geo, angles, niter, index, lmbda=1.0, noneg=True, callback=None):
+    """OS-SART with FP64 state over the oracle pair (Siddon Ax, FDK Atb):
+    W of set_w (iterative_recon_alg.py:214-230), V of set_v (:232-270), the per-subset update of
+    update_image (:372-401) and the clip of art_data_minimizing (:326-345).  index: the view
+    subsets in update order (order_subsets).  callback(it, x) after every iteration (FP64 x)."""
+    g = copy.deepcopy(geo)
+    g.check_geo(angles)
+    ang = np.asarray(g.angles, dtype=np.float64)
+    b = np.asarray(proj, dtype=np.float64)
+    parallel = getattr(g, "mode", "cone") == "parallel"
+
+    def sub(idx):
+        gs = copy.deepcopy(g)
+        for name in ("offOrigin", "offDetector", "rotDetector", "DSD", "DSO", "COR"):
+            setattr(gs, name, np.asarray(getattr(g, name))[idx])
+        gs.angles = ang[idx]
+        return gs
+
+    gx = copy.deepcopy(g)
+    sv = np.array(gx.sVoxel, dtype=np.float64)
+    sv[1:] = sv[1:] * 1.1
+    sv[0] = max(float(gx.sDetector[0]), sv[0])
+    gx.sVoxel, gx.nVoxel = sv, np.array([2, 2, 2])
+    gx.dVoxel = sv / gx.nVoxel
+    W = ax(np.ones((2, 2, 2), dtype=np.float32), gx, ang, "Siddon").astype(np.float64)
+    W[W <= min(np.asarray(g.dVoxel, dtype=np.float64) / 2)] = np.inf
+    W = 1.0 / W
+    nv, nu = int(g.nDetector[0]), int(g.nDetector[1])
+    shape = tuple(int(v) for v in g.nVoxel)
+    V = []
+    for idx in index:
+        idx = np.asarray(idx).reshape(-1)
+        if parallel:
+            v = np.full(shape[1:], float(len(idx)))
+        else:
+            gs = sub(idx)
+            s2 = np.array(gs.sVoxel, dtype=np.float64)
+            gs.sVoxel = s2 * np.max(s2[1:] / np.linalg.norm(s2[1:])) * 0.9
+            gs.dVoxel = gs.sVoxel / gs.nVoxel
+            v = atb(np.ones((len(idx), nv, nu), dtype=np.float32), gs, gs.angles, "FDK").astype(np.float64).mean(0)
+        v[v == 0.0] = np.inf
+        V.append(v)
+    x = np.zeros(shape, dtype=np.float64)
+    for it in range(niter):
+        for j, idx in enumerate(index):
+            idx = np.asarray(idx).reshape(-1)
+            gs = sub(idx)
+            est = ax(x.astype(np.float32), gs, gs.angles, "Siddon").astype(np.float64)
+            err = W[idx] * (b[idx] - est)
+            x = x + lmbda / V[j] * atb(err.astype(np.float32), gs, gs.angles, "FDK").astype(np.float64)
+            if noneg:
+                x[x < 0.0] = 0.0
+        if callback is not None:
+            callback(it, x)
+    return x.astype(np.float32)
+
+
 def _kry_ops(geo, angles):
     A = lambda v: ax(np.asarray(v, dtype=np.float32), geo, angles, "Siddon").astype(np.float64)  # noqa: E731
     At = lambda r: atb(np.asarray(r, dtype=np.float32), geo, angles, "matched").astype(np.float64)  # noqa: E731

@@ -128,3 +128,55 @@ def test_segment_counts_and_miss():
     g.offOrigin = np.array((500.0, 0.0, 0.0))
     p2 = O.ax(img, g, G.angles(2), "Siddon")
     assert np.all(p2 == 0)
+
+
+def test_rounding_oracle_nearest_bf16_matches_torch():
+    import torch
+    from oracle import rounding as R
+    v = (np.random.default_rng(0).standard_normal(50000) * 1e3).astype(np.float32)
+    v[:4] = [np.inf, -np.inf, 0.0, 1e-40]
+    want = torch.from_numpy(v).bfloat16().float().numpy()
+    np.testing.assert_array_equal(R.bf16_to_f32(R.bf16_bits_nearest(v)), want)
+
+
+@pytest.mark.parametrize("dtype", ["bfloat16", "float16"])
+def test_rounding_oracle_stochastic_picks_a_neighbour_without_bias(dtype):
+    from oracle import rounding as R
+    rng = np.random.default_rng(1)
+    v = rng.uniform(0.5, 4.0, (64, 1000)).astype(np.float32)
+    outs = np.stack([R.sart_update(v, np.zeros_like(v), np.ones(1000, np.float32), 1.0, False, dtype,
+                                   "stochastic", seed=3, step=k) for k in range(200)])
+    if dtype == "bfloat16":
+        lo = R.bf16_to_f32(((v.view(np.uint32) >> 16) << 16).astype(np.uint32) >> 16)
+        hi = R.bf16_to_f32((v.view(np.uint32) >> 16) + 1)
+    else:
+        h = v.astype(np.float16)
+        lo = np.where(h.astype(np.float32) > v, np.nextafter(h, np.float16(-np.inf)), h).astype(np.float32)
+        hi = np.where(h.astype(np.float32) < v, np.nextafter(h, np.float16(np.inf)), h).astype(np.float32)
+    exact = lo == v
+    assert np.all((outs == lo) | (outs == hi))
+    assert np.all(outs[:, exact] == v[exact])
+    # mean over 200 draws x 64000 values: unbiased to a few sigma of the pooled mean
+    d = (outs.astype(np.float64) - v).mean(0) / (hi - lo).astype(np.float64).clip(min=1e-30)
+    assert abs(d[~exact].mean()) < 5 * 0.5 / np.sqrt(200 * (~exact).sum())
+
+
+def test_rounding_oracle_random_bits_depend_on_step_and_seed():
+    from oracle import rounding as R
+    a = R.random16(3, 20, seed=1, step=0)
+    assert a.shape == (3, 20) and a.max() < 65536
+    assert not np.array_equal(a, R.random16(3, 20, seed=1, step=1))
+    assert not np.array_equal(a, R.random16(3, 20, seed=2, step=0))
+    # a plane of 16 voxels draws the same bits as the first 16 of a plane of 20 (groups of 8)
+    np.testing.assert_array_equal(a[0, :16], R.random16(1, 16, seed=1, step=0)[0])
+
+
+def test_oracle_ossart_reduces_error_and_keeps_nonnegativity():
+    geo = cone_geometry((16, 16, 16), (16.0,) * 3, (24, 32), (0.8, 0.8))
+    ang = G.angles(12)
+    img = G.phantom((16, 16, 16), seed=2)
+    proj = O.ax(img, geo, ang, "Siddon")
+    index = [np.arange(0, 6), np.arange(6, 12)]
+    errs = []
+    x = O.ossart(proj, geo, ang, 3, index, callback=lambda it, x: errs.append(np.linalg.norm(x - img)))
+    assert x.min() >= 0 and errs[0] < np.linalg.norm(img) and errs[-1] < errs[0]

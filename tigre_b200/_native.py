@@ -17,6 +17,7 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libtigre_b200.so")
 
 F32, BF16, F16 = 0, 1, 2
+ROUND_NEAREST, ROUND_STOCHASTIC = 0, 1
 PROJ_SIDDON, PROJ_INTERPOLATED = 0, 1
 BACKPROJ_FDK, BACKPROJ_MATCHED = 0, 1
 PLAN_PARALLEL = 1
@@ -99,6 +100,8 @@ _SIGS = {
                                    C.c_void_p, C.c_void_p]),
     "tigre_tv_piccs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_float,
                                  C.c_int, C.c_void_p, C.c_void_p]),
+    "tigre_sart_update": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_longlong,
+                                    C.c_longlong, C.c_int, C.c_ulonglong, C.c_ulonglong, C.c_void_p]),
     "tigre_noise_1d": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.c_float, C.c_float, C.c_ulonglong, C.c_void_p,
                                  C.c_void_p, C.c_int]),
     "tigre_add_noise": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_float, C.c_float,

@@ -32,6 +32,11 @@ class Problem:
             self.device = proj.device
             self.b = proj.detach().to(T.float32).contiguous()
         self.geo_in = geo
+        # checked at the caller's precision: geometries derived from this one (view subsets, the
+        # ART weight geometries) are re-checked by Ax/Atb, and a float32 copy of
+        # sDetector = nDetector * dDetector can miss check_geo's 1e-6 size test
+        self.geo_full = copy.deepcopy(geo)
+        self.geo_full.check_geo(angles)
         self.geo = N.checked_geometry(geo, angles)
         self.angles = np.ascontiguousarray(np.asarray(self.geo.angles, dtype=np.float32).reshape(-1, 3))
         self.n = self.angles.shape[0]
@@ -59,10 +64,10 @@ class Problem:
 
     def sub_geometry(self, index):
         """Geometry restricted to the views in `index` (art_data_minimizing, iterative_recon_alg.py:326-345)."""
-        g = copy.deepcopy(self.geo)
+        g = copy.deepcopy(self.geo_full)
         idx = np.asarray(index)
         for name in ("offOrigin", "offDetector", "rotDetector", "DSD", "DSO", "COR"):
-            setattr(g, name, np.asarray(getattr(self.geo, name))[idx])
+            setattr(g, name, np.asarray(getattr(self.geo_full, name))[idx])
         g.angles = self.angles[idx]
         return g
 

@@ -11,7 +11,12 @@ Per subset the forward projection, the weighted residual, the FDK
 backprojection and the update run on the GPU; subsets that are contiguous
 view ranges reuse the full plan (angle_range), others get their own plan.
 Storage precision (extension): storage=torch.bfloat16/float16 keeps the
-volume and the projections in that type (FP32 arithmetic, FP64 geometry).
+volume and the projections in that type (FP32 arithmetic, FP64 geometry);
+proj_storage= overrides the projections' type alone (torch.float32 keeps
+them exact); rounding="stochastic" (with seed=) rounds each volume update stochastically
+instead of to nearest, so updates below half a unit in the last place are
+kept in expectation.  The volume update itself is one fused kernel
+(tigre_sart_update).
 """
 from __future__ import annotations
 
@@ -26,9 +31,14 @@ from ._common import Problem, torch
 
 
 class ART:
-    def __init__(self, prob: Problem, blocksize, order=None, lmbda=1.0, noneg=True, storage=None, verbose=False):
+    def __init__(self, prob: Problem, blocksize, order=None, lmbda=1.0, noneg=True, storage=None, verbose=False,
+                 rounding="nearest", seed=0, proj_storage=None):
         T = torch()
+        proj_storage = storage if proj_storage is None else proj_storage
         self.prob = prob
+        self.rounding = rounding
+        self.seed = int(seed)
+        self.step = 0
         self.lmbda = float(lmbda)
         self.noneg = noneg
         self.verbose = verbose
@@ -46,12 +56,12 @@ class ART:
             else:
                 sub = prob.sub_geometry(idx)
                 self.plans.append((N.get_plan(N.checked_geometry(sub, sub.angles), prob.device.index), None))
-        self.b = prob.b.to(self.storage) if self.storage != T.float32 else prob.b
+        self.b = prob.b.to(proj_storage) if proj_storage not in (None, T.float32) else prob.b
 
     def _weights_w(self):
         T = torch()
         prob = self.prob
-        gx = copy.deepcopy(prob.geo)
+        gx = copy.deepcopy(prob.geo_full)
         gx.sVoxel = np.array(gx.sVoxel, dtype=np.float64)
         gx.sVoxel[1:] = gx.sVoxel[1:] * 1.1
         gx.sVoxel[0] = max(float(gx.sDetector[0]), gx.sVoxel[0])
@@ -59,7 +69,7 @@ class ART:
         gx.dVoxel = gx.sVoxel / gx.nVoxel
         plan = N.get_plan(N.checked_geometry(gx, prob.angles), prob.device.index)
         W = P.ax(T.ones((2, 2, 2), dtype=T.float32, device=prob.device), plan, "Siddon")
-        W[W <= float(min(np.asarray(prob.geo.dVoxel) / 2))] = float("inf")
+        W[W <= float(min(np.asarray(prob.geo_full.dVoxel, dtype=np.float64) / 2))] = float("inf")
         return 1.0 / W
 
     def _weights_v(self):
@@ -68,6 +78,10 @@ class ART:
         g = prob.geo
         V = []
         for idx in self.index:
+            if getattr(g, "mode", "cone") == "parallel":   # set_v: V = block length (:265-266)
+                V.append(T.full(tuple(int(v) for v in g.nVoxel[1:]), float(len(idx)), dtype=T.float32,
+                                device=prob.device))
+                continue
             gx = prob.sub_geometry(idx)
             sv = np.array(gx.sVoxel, dtype=np.float64)
             gx.sVoxel = sv * np.max(sv[1:] / np.linalg.norm(sv[1:])) * 0.9
@@ -95,10 +109,8 @@ class ART:
                 est = P.ax(x, plan, "Siddon", out_dtype=T.float32)
             err = (w_j * (b_j.float() - est)).contiguous()
             bp = P.atb(err, plan, "FDK", angle_range=rng, out_dtype=T.float32)
-            upd = x.float() + (self.lmbda / self.V[j]).unsqueeze(0) * bp
-            if self.noneg:
-                upd.clamp_(min=0)
-            x.copy_(upd)
+            P.sart_update_(x, bp, self.V[j], self.lmbda, self.noneg, self.rounding, self.seed, self.step)
+            self.step += 1
         return x
 
 
@@ -107,7 +119,8 @@ def _run(proj, geo, angles, niter, blocksize, kwargs):
     T = torch()
     storage = kwargs.get("storage", None)
     art = ART(prob, blocksize, kwargs.get("OrderStrategy"), kwargs.get("lmbda", 1.0), kwargs.get("noneg", True),
-              storage, kwargs.get("verbose", False))
+              storage, kwargs.get("verbose", False), kwargs.get("rounding", "nearest"), kwargs.get("seed", 0),
+              kwargs.get("proj_storage"))
     init = kwargs.get("init", None)
     if isinstance(init, str) and init == "FDK":
         from .single_pass import fdk_device

@@ -20,37 +20,11 @@
 #include <cmath>
 #include <cstdint>
 
+#include "philox.cuh"
 #include "tigre_internal.h"
 
 namespace tigre {
 namespace {
-
-struct U4 {
-    uint32_t x, y, z, w;
-};
-
-__host__ __device__ __forceinline__ void mulhilo(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo) {
-    const uint64_t p = (uint64_t)a * (uint64_t)b;
-    hi = (uint32_t)(p >> 32);
-    lo = (uint32_t)p;
-}
-
-// Philox4x32 with 10 rounds: multipliers 0xD2511F53 / 0xCD9E8D57, key increments
-// 0x9E3779B9 / 0xBB67AE85 (the published constants of the SC 2011 paper).
-__host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
-#pragma unroll
-    for (int r = 0; r < 10; ++r) {
-        if (r > 0) {
-            k0 += 0x9E3779B9u;
-            k1 += 0xBB67AE85u;
-        }
-        uint32_t hi0, lo0, hi1, lo1;
-        mulhilo(0xD2511F53u, c.x, hi0, lo0);
-        mulhilo(0xCD9E8D57u, c.z, hi1, lo1);
-        c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
-    }
-    return c;
-}
 
 // uniform in (0, 1): 24 random bits at the centre of their cell (exact in FP32)
 __device__ __forceinline__ float u01f(uint32_t x) { return ((float)(x >> 8) + 0.5f) * (1.0f / 16777216.0f); }

@@ -134,6 +134,28 @@ def tv_piccs_(vol: torch.Tensor, prior: torch.Tensor, alpha: float, ratio: float
     return vol
 
 
+def sart_update_(x: torch.Tensor, bp: torch.Tensor, v: torch.Tensor, lmbda: float, noneg: bool = True,
+                 rounding: str = "nearest", seed: int = 0, step: int = 0):
+    """In place x <- max(x + (lmbda / v) * bp, 0) on a device volume (tigre_sart_update).
+    x: (nz, ny, nx) float32/bfloat16/float16; bp: float32 like x; v: float32 (ny, nx).
+    rounding "stochastic" rounds 16-bit storage with Philox bits of (seed, step, voxel)."""
+    if x.dim() != 3 or not x.is_cuda or not x.is_contiguous():
+        raise ValueError("expected a contiguous CUDA volume (nZ, nY, nX)")
+    nz, ny, nx = x.shape
+    if bp.dtype != torch.float32 or tuple(bp.shape) != tuple(x.shape) or not bp.is_contiguous():
+        raise ValueError("bp must be a contiguous float32 volume shaped like x")
+    if v.dtype != torch.float32 or tuple(v.shape) != (ny, nx) or not v.is_contiguous():
+        raise ValueError("v must be a contiguous float32 (ny, nx) plane")
+    if bp.device != x.device or v.device != x.device:
+        raise ValueError("x, bp and v must be on one device")
+    mode = {"nearest": N.ROUND_NEAREST, "stochastic": N.ROUND_STOCHASTIC}[rounding]
+    N.check(N.lib().tigre_sart_update(C.c_void_p(x.data_ptr()), _dt(x), C.c_void_p(bp.data_ptr()),
+                                      C.c_void_p(v.data_ptr()), float(lmbda), 1 if noneg else 0, nz, ny * nx, mode,
+                                      int(seed) & (2 ** 64 - 1), int(step) & (2 ** 64 - 1), _stream(x)),
+            "tigre_sart_update")
+    return x
+
+
 def tv_gradient(vol: torch.Tensor, out: torch.Tensor = None):
     nx, ny, nz = _vol3(vol)
     if out is None:
