@@ -40,6 +40,7 @@ NVOX = (512, 512, 512)
 DDET, SVOL = 0.4, 256.0
 METRIC = "GRays/s Ax + Gvox-upd/s Atb at 512^3"
 WORKLOAD = "cone-beam 512^3 @ 0.5 mm, 1024x768 det @ 0.4 mm, 720 views / 2pi, DSO 1000, DSD 1536"
+TV_ALPHA, TV_ITERS = 0.002, 20   # POCS-TV timing: 20 descent steps on the phantom volume
 
 
 def set_size(size, views):
@@ -204,6 +205,9 @@ def run_reference(args, rank):
         _, t_fdk = ref.atb(proj, geo, ang, "FDK", repeat=2)
         ops["atb_fdk_f32"] = {"value": round(upd / t_fdk[-1] / 1e9, 4), "unit": "Gvox-upd/s",
                               "ms_per_call": round(1e3 * t_fdk[-1], 3)}
+        _, t_tv = ref.pocs_tv(img, TV_ALPHA, TV_ITERS, repeat=2)
+        ops["tv_pocs_f32_e2e"] = {"value": round(math.prod(NVOX) * TV_ITERS / t_tv[-1] / 1e9, 4),
+                                  "unit": "Gvox-iter/s", "ms_per_call": round(1e3 * t_tv[-1], 3)}
         line["ops"] = ops
     print(json.dumps(line))
 
@@ -362,6 +366,9 @@ def time_ops(P, plan, vol, proj, reps=3):
         "atb_matched_bf16": (lambda: P.atb(proj16, plan, "matched", out=v16_out), upd, "Gvox-upd/s"),
         "atb_fdk_bf16": (lambda: P.atb(proj16, plan, "FDK", out=v16_out), upd, "Gvox-upd/s"),
     }
+    tv_vol, tv_work = vol.clone(), torch.empty_like(vol)
+    cases["tv_pocs_f32"] = (lambda: P.tv_pocs_(tv_vol, TV_ALPHA, TV_ITERS, tv_work), math.prod(NVOX) * TV_ITERS,
+                            "Gvox-iter/s")
     out = {}
     for name, (fn, units, unit) in cases.items():
         fn()
@@ -374,7 +381,16 @@ def time_ops(P, plan, vol, proj, reps=3):
         torch.cuda.synchronize()
         dt = e0.elapsed_time(e1) / 1e3 / reps
         out[name] = {"value": round(units / dt / 1e9, 4), "unit": unit, "ms_per_launch": round(1e3 * dt, 3)}
-    del vol16, proj16, p_out, v_out, p16_out, v16_out
+    del vol16, proj16, p_out, v_out, p16_out, v16_out, tv_vol, tv_work
+    # POCS-TV through the host API (numpy in and out, copies included), as minTV is called
+    from tigre_b200.utilities.minTV import minTV
+    host = vol.cpu().numpy()
+    minTV(host, TV_ALPHA, TV_ITERS)
+    t = time.perf_counter()
+    minTV(host, TV_ALPHA, TV_ITERS)
+    dt = time.perf_counter() - t
+    out["tv_pocs_f32_e2e"] = {"value": round(math.prod(NVOX) * TV_ITERS / dt / 1e9, 4), "unit": "Gvox-iter/s",
+                              "ms_per_call": round(1e3 * dt, 3)}
     return out
 
 

@@ -6,8 +6,8 @@
 // The reference runs gradientTV, a device copy, two reduction kernels, a host
 // synchronisation and three element-wise kernels per step (~48 B/voxel).
 // Here a step is two passes and no host round trip (~12 B/voxel):
-//   pass 1  tv_norm_kernel    stencil -> g, sum g^2 (FP64, one atomic per block)
-//   pass 2  tv_update_kernel  stencil again -> g, writes f - alpha g / |g|,
+//   pass 1  tv_tiled_kernel<kTvOutNorm>    stencil -> g, sum g^2 (FP64, one atomic per block)
+//   pass 2  tv_tiled_kernel<kTvOutUpdate>  stencil again -> g, writes f - alpha g / |g|,
 //                             reading |g|^2 from device memory (ping-pong buffers)
 // g is recomputed rather than stored: the stencil is cheap, the bytes are not.
 //
@@ -19,6 +19,7 @@
 #include <cmath>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "tigre_internal.h"
 
@@ -29,45 +30,21 @@ struct TVDims {
     int nx, ny, nz;
 };
 
+// Voxels (x, y, z < nzr) of the per-voxel kernels: blocks stride over (y, z) rows, threads over
+// x, so no thread divides a linear index; i is the linear index of (x, y, z).
+#define TV_FOR_EACH_VOXEL(d, nzr, x, y, z, i)                                                     \
+    for (long row_ = blockIdx.x; row_ < (long)(d).ny * (nzr); row_ += gridDim.x) {               \
+        const int y = (int)(row_ % (d).ny), z = (int)(row_ / (d).ny);                             \
+        for (int x = threadIdx.x; x < (d).nx; x += blockDim.x) {                                   \
+            const size_t i = ((size_t)z * (d).ny + y) * (d).nx + x;
+#define TV_END_FOR_EACH_VOXEL \
+    }                         \
+    }
+
+int grid_rows(const TVDims& d, int nzr) { return (int)std::min<long>((long)d.ny * nzr, 148 * 16); }
+
 __device__ __forceinline__ float fget(const float* __restrict__ f, const TVDims& d, int x, int y, int z) {
     return (z >= 0 && z < d.nz) ? __ldg(f + ((size_t)z * d.ny + y) * d.nx + x) : 0.f;
-}
-
-// dftv of GD_TV.cu:135-140 at (x,y,z); eps 1e-8 as the reference.
-__device__ __forceinline__ float tv_grad_at(const float* __restrict__ f, const TVDims& d, int x, int y, int z) {
-    const float eps = 1e-8f;
-    const float c = fget(f, d, x, y, z);
-    const float cxm = x > 0 ? fget(f, d, x - 1, y, z) : 0.f;
-    const float cym = y > 0 ? fget(f, d, x, y - 1, z) : 0.f;
-    const float czm = fget(f, d, x, y, z - 1);
-    // backward differences at the voxel itself
-    const float d0 = c - czm;
-    const float d1 = y > 0 ? c - cym : 0.f;
-    const float d2 = x > 0 ? c - cxm : 0.f;
-    float g = (d0 + d1 + d2) / (sqrtf(d0 * d0 + d1 * d1 + d2 * d2) + eps);
-    if (x + 1 < d.nx) {   // neighbour (x+1): its x difference involves f(x)
-        const float n = fget(f, d, x + 1, y, z);
-        const float e0 = n - fget(f, d, x + 1, y, z - 1);
-        const float e1 = y > 0 ? n - fget(f, d, x + 1, y - 1, z) : 0.f;
-        const float e2 = n - c;
-        g -= e2 / (sqrtf(e0 * e0 + e1 * e1 + e2 * e2) + eps);
-    }
-    if (y + 1 < d.ny) {
-        const float n = fget(f, d, x, y + 1, z);
-        const float e0 = n - fget(f, d, x, y + 1, z - 1);
-        const float e1 = n - c;
-        const float e2 = x > 0 ? n - fget(f, d, x - 1, y + 1, z) : 0.f;
-        g -= e1 / (sqrtf(e0 * e0 + e1 * e1 + e2 * e2) + eps);
-    }
-    {   // neighbour (z+1); above the last slice it is the zero halo slice
-        const float n = fget(f, d, x, y, z + 1);
-        const bool inside = z + 1 < d.nz;
-        const float e0 = n - c;
-        const float e1 = (inside && y > 0) ? n - fget(f, d, x, y - 1, z + 1) : 0.f;
-        const float e2 = (inside && x > 0) ? n - fget(f, d, x - 1, y, z + 1) : 0.f;
-        g -= e0 / (sqrtf(e0 * e0 + e1 * e1 + e2 * e2) + eps);
-    }
-    return g;
 }
 
 __device__ __forceinline__ double block_sum(double v) {
@@ -87,54 +64,174 @@ __device__ __forceinline__ double block_sum(double v) {
     return v;
 }
 
-// grid-stride over voxels, x fastest
-__global__ void __launch_bounds__(256) tv_norm_kernel(const float* __restrict__ f, TVDims d, double* __restrict__ out) {
-    const size_t n = (size_t)d.nx * d.ny * d.nz;
-    double s = 0.0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % d.nx);
-        const size_t r = i / d.nx;
-        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
-        const float g = tv_grad_at(f, d, x, y, z);
-        s += (double)g * (double)g;
-    }
-    s = block_sum(s);
-    if (threadIdx.x == 0) atomicAdd(out, s);
+// ---- tiled gradientTV: the POCS passes and the autograd gradient ----
+//
+// A block owns a 32 x 8 tile of (x, y) columns and marches down a chunk of kTvZC slices.
+// Per slice it stages f with a one-voxel x/y halo in shared memory and computes, at every
+// tile point and at the tile's +x column and +y row, the backward differences (dz, dy, dx)
+// and r = 1 / (sqrt(dz^2 + dy^2 + dx^2) + 1e-8) of gradientTV (GD_TV.cu:117-143).  The
+// gradient at (x, y, z) (dftv, GD_TV.cu:135-140) is then
+//     (dz + dy + dx) r  -  dx(x+1) r(x+1)  -  dy(y+1) r(y+1)  -  dz(z+1) r(z+1),
+// with each norm evaluated once instead of four times and each voxel read from global memory
+// once per slice (plus the halo), with no integer division per voxel.  The differences are
+// the reference's exactly; r uses the hardware reciprocal square root and reciprocal, so each
+// term carries a relative error of a few 1e-7 against the reference's IEEE divisions.
+// Zero-filled staging reproduces the boundary rule: the zero slices below z = 0 and above
+// z = nz - 1, and zero differences across the -x / -y faces.
+//
+// Pipeline: staged slices live in a ring of three buffers and the (dy, dx, r) planes in two,
+// so one barrier per slice suffices; each thread fetches its staged elements three slices
+// ahead into registers, so global loads overlap the arithmetic of the slices before them.
+constexpr int kTvTX = 32, kTvTY = 8, kTvZC = 32;
+constexpr int kTvFX = kTvTX + 2, kTvFY = kTvTY + 2;   // staged f: x0-1 .. x0+32, y0-1 .. y0+8
+constexpr int kTvQX = kTvTX + 1, kTvQY = kTvTY + 1;   // difference points: x0 .. x0+32, y0 .. y0+8
+constexpr int kTvOutNorm = 0, kTvOutUpdate = 1, kTvOutGrad = 2;
+
+struct TvTiles {
+    int tx, ty, tz, ntiles;
+};
+
+TvTiles tv_tiles(const TVDims& d) {
+    TvTiles t{(d.nx + kTvTX - 1) / kTvTX, (d.ny + kTvTY - 1) / kTvTY, (d.nz + kTvZC - 1) / kTvZC, 0};
+    t.ntiles = t.tx * t.ty * t.tz;
+    return t;
 }
 
-__global__ void __launch_bounds__(256) tv_update_kernel(const float* __restrict__ f, float* __restrict__ o, TVDims d,
-                                                        const double* __restrict__ sumsq, float alpha) {
-    const size_t n = (size_t)d.nx * d.ny * d.nz;
-    // reference: |g| = sqrt(sum + 1e-7), then g/|g| * alpha (GD_TV.cu:561-580)
-    const float scale = (float)((double)alpha / sqrt(*sumsq + 1e-7));
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % d.nx);
-        const size_t r = i / d.nx;
-        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
-        const float g = tv_grad_at(f, d, x, y, z);
-        o[i] = fmaf(-scale, g, __ldg(f + i));
-    }
+int tv_tiled_grid(const TvTiles& t) { return std::min(t.ntiles, 148 * 8); }
+
+// 1 / (sqrt(s) + eps) for s >= 0
+__device__ __forceinline__ float tv_rnorm(float s) {
+    const float q = s > 0.f ? s * rsqrtf(s) : 0.f;
+    return __fdividef(1.f, q + 1e-8f);
 }
 
-__global__ void __launch_bounds__(256) tv_grad_kernel(const float* __restrict__ f, float* __restrict__ o, TVDims d) {
-    const size_t n = (size_t)d.nx * d.ny * d.nz;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % d.nx);
-        const size_t r = i / d.nx;
-        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
-        o[i] = tv_grad_at(f, d, x, y, z);
+// OUT: kTvOutNorm adds sum g^2 (FP64, one atomic per block) into *sums; kTvOutUpdate writes
+// o = f - alpha g / sqrt(*sums + 1e-7) (GD_TV.cu:556-597); kTvOutGrad writes o = g.
+template <int OUT>
+__global__ void __launch_bounds__(256) tv_tiled_kernel(const float* __restrict__ f, float* __restrict__ o, TVDims d,
+                                                       TvTiles T, double* __restrict__ sums, float alpha) {
+    constexpr int FS = kTvFY * kTvFX;   // one staged slice
+    __shared__ float F[3 * FS];
+    // dy, dx and r of a staged slice (dz is needed only at a thread's own column: registers)
+    __shared__ float Qy[2][kTvQY][kTvQX], Qx[2][kTvQY][kTvQX], Qr[2][kTvQY][kTvQX];
+    const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5;
+    float scale = 0.f;
+    if (OUT == kTvOutUpdate) scale = (float)((double)alpha / sqrt(*sums + 1e-7));
+    const int plane = d.nx * d.ny;   // the host keeps nx * ny * nz below 2^31
+    // the +x column (qx = 32, qy = 0..8) and the +y row (qy = 8) of difference points
+    const bool extra = tid < kTvQY + kTvTX;
+    const int eqx = tid < kTvQY ? kTvTX : tid - kTvQY, eqy = tid < kTvQY ? tid : kTvTY;
+    double acc = 0.0;
+    for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
+        const int bx = t % T.tx, rt = t / T.tx;
+        const int by = rt % T.ty, bz = rt / T.ty;
+        const int x0 = bx * kTvTX, y0 = by * kTvTY, z0 = bz * kTvZC;
+        const int zend = min(z0 + kTvZC, d.nz);   // output slices z0 .. zend-1; slice zend supplies dz(z+1)
+        // thread tid stages elements k = tid and k = tid + 256 (k < 340) of every slice; their
+        // in-slice offsets are fixed per tile (-1 outside the volume: zero)
+        int off[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int k = tid + 256 * j;
+            const int fy = k / kTvFX, fx = k - fy * kTvFX;
+            const int xx = x0 - 1 + fx, yy = y0 - 1 + fy;
+            off[j] = (k < FS && xx >= 0 && xx < d.nx && yy >= 0 && yy < d.ny) ? yy * d.nx + xx : -1;
+        }
+        auto fetch = [&](int zz, float (&v)[2]) {
+            const bool zin = zz >= 0 && zz < d.nz;
+#pragma unroll
+            for (int j = 0; j < 2; ++j) v[j] = (zin && off[j] >= 0) ? __ldg(f + (zz * plane + off[j])) : 0.f;
+        };
+        auto put = [&](int slot, const float (&v)[2]) {
+            F[slot * FS + tid] = v[0];
+            if (tid + 256 < FS) F[slot * FS + tid + 256] = v[1];
+        };
+        // differences and reciprocal norm at point (qx, qy) of slice slot sc over slice slot sp
+        auto qpoint = [&](int qx, int qy, int sc, int sp, float& dz, float& dy, float& dx) {
+            const int k = (qy + 1) * kTvFX + qx + 1;
+            const float c = F[sc * FS + k];
+            dz = c - F[sp * FS + k];
+            dy = y0 + qy > 0 ? c - F[sc * FS + k - kTvFX] : 0.f;
+            dx = x0 + qx > 0 ? c - F[sc * FS + k - 1] : 0.f;
+            return tv_rnorm(dz * dz + dy * dy + dx * dx);
+        };
+        const int x = x0 + lx, y = y0 + ly;
+        const bool inside = x < d.nx && y < d.ny;
+        const int own = y * d.nx + x;
+        // R[j]: registers holding a fetched slice; at relative step j the slice zz + 1 is in
+        // R[(j + 1) % 3] and slice zz + 3 is fetched into R[j % 3]
+        float R[3][2];
+        fetch(z0 - 1, R[0]);
+        put(0, R[0]);
+        fetch(z0, R[0]);
+        put(1, R[0]);
+        fetch(z0 + 1, R[1]);
+        fetch(z0 + 2, R[2]);
+        __syncthreads();
+        float part = 0.f, fown = 0.f;
+        // one slice: slots (SP, SC, SN) hold slices zz - 1, zz, zz + 1; QB is the difference buffer
+        auto step = [&](int zz, auto SPc, auto SCc, auto SNc, auto QBc, auto RPc) {
+            constexpr int SP = decltype(SPc)::value, SC = decltype(SCc)::value, SN = decltype(SNc)::value;
+            constexpr int QB = decltype(QBc)::value, RP = decltype(RPc)::value;
+            if (zz + 1 <= zend) put(SN, R[RP]);
+            if (zz + 3 <= zend) fetch(zz + 3, R[(RP + 2) % 3]);
+            float dz, dy, dx;
+            const float r = qpoint(lx, ly, SC, SP, dz, dy, dx);
+            Qy[QB][ly][lx] = dy; Qx[QB][ly][lx] = dx; Qr[QB][ly][lx] = r;
+            if (extra) {
+                float a, b, c;
+                const float m = qpoint(eqx, eqy, SC, SP, a, b, c);
+                Qy[QB][eqy][eqx] = b; Qx[QB][eqy][eqx] = c; Qr[QB][eqy][eqx] = m;
+            }
+            __syncthreads();
+            if (zz > z0 && inside) {   // slice zz-1 is complete with its +z neighbour's term
+                const float g = part - dz * r;
+                if (OUT == kTvOutNorm) acc += (double)g * (double)g;
+                else {
+                    const int i = (zz - 1) * plane + own;
+                    o[i] = OUT == kTvOutUpdate ? fmaf(-scale, g, fown) : g;
+                }
+            }
+            if (zz < zend && inside) {
+                float g = (dz + dy + dx) * r;
+                if (x + 1 < d.nx) g -= Qx[QB][ly][lx + 1] * Qr[QB][ly][lx + 1];
+                if (y + 1 < d.ny) g -= Qy[QB][ly + 1][lx] * Qr[QB][ly + 1][lx];
+                part = g;
+                fown = F[SC * FS + (ly + 1) * kTvFX + lx + 1];
+            }
+        };
+        using I0 = std::integral_constant<int, 0>;
+        using I1 = std::integral_constant<int, 1>;
+        using I2 = std::integral_constant<int, 2>;
+        // six relative steps bring the three slots, two buffers and three register pairs back to
+        // their starting assignment
+        for (int zb = z0; zb <= zend; zb += 6) {
+            step(zb, I0{}, I1{}, I2{}, I0{}, I1{});
+            if (zb + 1 > zend) break;
+            step(zb + 1, I1{}, I2{}, I0{}, I1{}, I2{});
+            if (zb + 2 > zend) break;
+            step(zb + 2, I2{}, I0{}, I1{}, I0{}, I0{});
+            if (zb + 3 > zend) break;
+            step(zb + 3, I0{}, I1{}, I2{}, I1{}, I1{});
+            if (zb + 4 > zend) break;
+            step(zb + 4, I1{}, I2{}, I0{}, I0{}, I2{});
+            if (zb + 5 > zend) break;
+            step(zb + 5, I2{}, I0{}, I1{}, I1{}, I0{});
+        }
+        __syncthreads();   // the next tile restages the ring
+    }
+    if (OUT == kTvOutNorm) {
+        acc = block_sum(acc);
+        if (threadIdx.x == 0) atomicAdd(sums, acc);
     }
 }
 
 // sum_i |grad f_i| over the voxels and the zero halo slice above the last one
-// (whose gradient norm is |f(x,y,nz-1)|); its derivative is tv_grad_at.
+// (whose gradient norm is |f(x,y,nz-1)|); its derivative is the gradient of tv_tiled_kernel.
 __global__ void __launch_bounds__(256) tv_value_kernel(const float* __restrict__ f, TVDims d, double* __restrict__ out) {
-    const size_t n = (size_t)d.nx * d.ny * (d.nz + 1);
     double s = 0.0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % d.nx);
-        const size_t r = i / d.nx;
-        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
+    TV_FOR_EACH_VOXEL(d, d.nz + 1, x, y, z, i) {
+        (void)i;
         if (z == d.nz) {
             s += fabs((double)fget(f, d, x, y, z - 1));
             continue;
@@ -145,6 +242,7 @@ __global__ void __launch_bounds__(256) tv_value_kernel(const float* __restrict__
         const float d2 = x > 0 ? c - fget(f, d, x - 1, y, z) : 0.f;
         s += sqrt((double)d0 * d0 + (double)d1 * d1 + (double)d2 * d2);
     }
+    TV_END_FOR_EACH_VOXEL
     s = block_sum(s);
     if (threadIdx.x == 0) atomicAdd(out, s);
 }
@@ -232,15 +330,13 @@ __device__ __forceinline__ float tv_step_grad(const float* __restrict__ f, const
 template <int KIND>
 __global__ void __launch_bounds__(256) tv_step_norm_kernel(const float* __restrict__ f, TVDims d, TVStep st,
                                                            double* __restrict__ out) {
-    const size_t n = (size_t)d.nx * d.ny * d.nz;
     double s = 0.0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % d.nx);
-        const size_t r = i / d.nx;
-        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
+    TV_FOR_EACH_VOXEL(d, d.nz, x, y, z, i) {
+        (void)i;
         const float g = tv_step_grad<KIND>(f, d, st, x, y, z);
         s += (double)g * (double)g;
     }
+    TV_END_FOR_EACH_VOXEL
     s = block_sum(s);
     if (threadIdx.x == 0) atomicAdd(out, s);
 }
@@ -249,20 +345,12 @@ template <int KIND>
 __global__ void __launch_bounds__(256) tv_step_update_kernel(const float* __restrict__ f, float* __restrict__ o,
                                                              TVDims d, TVStep st, const double* __restrict__ sumsq,
                                                              float alpha) {
-    const size_t n = (size_t)d.nx * d.ny * d.nz;
     const float scale = (float)((double)alpha / sqrt(*sumsq + st.norm_eps));
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % d.nx);
-        const size_t r = i / d.nx;
-        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
+    TV_FOR_EACH_VOXEL(d, d.nz, x, y, z, i) {
         const float g = tv_step_grad<KIND>(f, d, st, x, y, z);
         o[i] = fmaf(-scale, g, __ldg(f + i));
     }
-}
-
-int grid_for(size_t n) {
-    const size_t want = (n + 255) / 256;
-    return (int)std::min<size_t>(want, 148 * 16);
+    TV_END_FOR_EACH_VOXEL
 }
 
 }  // namespace
@@ -276,8 +364,9 @@ int tigre_tv_gradient(const void* d_img, int dtype, float* d_grad, long nx, long
     if (dtype != TIGRE_F32) return fail(TIGRE_ERR_BAD_ASSERT, "TV kernels take float32 volumes");
     if (nx <= 0 || ny <= 0 || nz <= 0 || !d_img || !d_grad) return fail(TIGRE_ERR_BAD_ASSERT, "bad TV arguments");
     TVDims d{(int)nx, (int)ny, (int)nz};
-    const size_t n = (size_t)nx * ny * nz;
-    tv_grad_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const float*)d_img, d_grad, d);
+    const TvTiles T = tv_tiles(d);
+    tv_tiled_kernel<kTvOutGrad><<<tv_tiled_grid(T), 256, 0, (cudaStream_t)stream>>>((const float*)d_img, d_grad, d, T,
+                                                                                     nullptr, 0.f);
     TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
@@ -286,8 +375,7 @@ int tigre_tv_value(const void* d_img, int dtype, long nx, long ny, long nz, doub
     if (dtype != TIGRE_F32) return fail(TIGRE_ERR_BAD_ASSERT, "TV kernels take float32 volumes");
     if (nx <= 0 || ny <= 0 || nz <= 0 || !d_img || !d_out) return fail(TIGRE_ERR_BAD_ASSERT, "bad TV arguments");
     TVDims d{(int)nx, (int)ny, (int)nz};
-    const size_t n = (size_t)nx * ny * (nz + 1);
-    tv_value_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>((const float*)d_img, d, d_out);
+    tv_value_kernel<<<grid_rows(d, d.nz + 1), 256, 0, (cudaStream_t)stream>>>((const float*)d_img, d, d_out);
     TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
@@ -308,9 +396,11 @@ int tigre_tv_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha
     TIGRE_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)std::max(max_iter, 1), st));
     float* cur = (float*)d_img;
     float* nxt = d_work;
+    const TvTiles T = tv_tiles(d);
+    const int grid = tv_tiled_grid(T);
     for (int it = 0; it < max_iter; ++it) {
-        tv_norm_kernel<<<grid_for(n), 256, 0, st>>>(cur, d, sums + it);
-        tv_update_kernel<<<grid_for(n), 256, 0, st>>>(cur, nxt, d, sums + it, alpha);
+        tv_tiled_kernel<kTvOutNorm><<<grid, 256, 0, st>>>(cur, nullptr, d, T, sums + it, 0.f);
+        tv_tiled_kernel<kTvOutUpdate><<<grid, 256, 0, st>>>(cur, nxt, d, T, sums + it, alpha);
         std::swap(cur, nxt);
     }
     if (cur != (float*)d_img) TIGRE_CUDA(cudaMemcpyAsync(d_img, cur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
@@ -334,8 +424,8 @@ static int tv_descent(void* d_img, long nx, long ny, long nz, float alpha, int m
     float* cur = (float*)d_img;
     float* nxt = d_work;
     for (int it = 0; it < max_iter; ++it) {
-        tv_step_norm_kernel<KIND><<<grid_for(n), 256, 0, st>>>(cur, d, stp, sums + it);
-        tv_step_update_kernel<KIND><<<grid_for(n), 256, 0, st>>>(cur, nxt, d, stp, sums + it, alpha);
+        tv_step_norm_kernel<KIND><<<grid_rows(d, d.nz), 256, 0, st>>>(cur, d, stp, sums + it);
+        tv_step_update_kernel<KIND><<<grid_rows(d, d.nz), 256, 0, st>>>(cur, nxt, d, stp, sums + it, alpha);
         std::swap(cur, nxt);
     }
     if (cur != (float*)d_img) TIGRE_CUDA(cudaMemcpyAsync(d_img, cur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
@@ -433,9 +523,11 @@ extern "C" int tigre_tv_pocs_noalloc(void* d_img, int dtype, long nx, long ny, l
     if (max_iter > 0) TIGRE_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)max_iter, st));
     float* cur = (float*)d_img;
     float* nxt = d_work;
+    const TvTiles T = tv_tiles(d);
+    const int grid = tv_tiled_grid(T);
     for (int it = 0; it < max_iter; ++it) {
-        tv_norm_kernel<<<grid_for(n), 256, 0, st>>>(cur, d, sums + it);
-        tv_update_kernel<<<grid_for(n), 256, 0, st>>>(cur, nxt, d, sums + it, alpha);
+        tv_tiled_kernel<kTvOutNorm><<<grid, 256, 0, st>>>(cur, nullptr, d, T, sums + it, 0.f);
+        tv_tiled_kernel<kTvOutUpdate><<<grid, 256, 0, st>>>(cur, nxt, d, T, sums + it, alpha);
         std::swap(cur, nxt);
     }
     if (cur != (float*)d_img) TIGRE_CUDA(cudaMemcpyAsync(d_img, cur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
