@@ -17,6 +17,7 @@
 // and the terms of neighbours beyond the last x / y index vanish.
 
 #include <cmath>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <type_traits>
@@ -82,22 +83,29 @@ __device__ __forceinline__ double block_sum(double v) {
 // Pipeline: staged slices live in a ring of three buffers and the (dy, dx, r) planes in two,
 // so one barrier per slice suffices; each thread fetches its staged elements three slices
 // ahead into registers, so global loads overlap the arithmetic of the slices before them.
-constexpr int kTvTX = 32, kTvTY = 8, kTvZC = 32;
-constexpr int kTvFX = kTvTX + 2, kTvFY = kTvTY + 2;   // staged f: x0-1 .. x0+32, y0-1 .. y0+8
-constexpr int kTvQX = kTvTX + 1, kTvQY = kTvTY + 1;   // difference points: x0 .. x0+32, y0 .. y0+8
+constexpr int kTvTX = 32, kTvZC = 32;   // tile width; slices per chunk (tile height: 8 rows per thread row)
+constexpr int kTvFX = kTvTX + 2;         // staged f: x0-1 .. x0+32 (and y0-1 .. y0+TY)
+constexpr int kTvQX = kTvTX + 1;         // difference points: x0 .. x0+32 (and y0 .. y0+TY)
 constexpr int kTvOutNorm = 0, kTvOutUpdate = 1, kTvOutGrad = 2;
 
 struct TvTiles {
     int tx, ty, tz, ntiles;
 };
 
-TvTiles tv_tiles(const TVDims& d) {
-    TvTiles t{(d.nx + kTvTX - 1) / kTvTX, (d.ny + kTvTY - 1) / kTvTY, (d.nz + kTvZC - 1) / kTvZC, 0};
+TvTiles tv_tiles(const TVDims& d, int rows) {
+    const int TY = 8 * rows;
+    TvTiles t{(d.nx + kTvTX - 1) / kTvTX, (d.ny + TY - 1) / TY, (d.nz + kTvZC - 1) / kTvZC, 0};
     t.ntiles = t.tx * t.ty * t.tz;
     return t;
 }
 
 int tv_tiled_grid(const TvTiles& t) { return std::min(t.ntiles, 148 * 8); }
+
+// rows of the tile each thread owns (1: 32 x 8 tiles, 2: 32 x 16); TIGRE_B200_TV_ROWS overrides
+int tv_rows() {
+    const char* e = std::getenv("TIGRE_B200_TV_ROWS");
+    return (e && std::atoi(e) == 1) ? 1 : (e && std::atoi(e) == 2) ? 2 : 2;
+}
 
 // 1 / (sqrt(s) + eps) for s >= 0
 __device__ __forceinline__ float tv_rnorm(float s) {
@@ -107,44 +115,48 @@ __device__ __forceinline__ float tv_rnorm(float s) {
 
 // OUT: kTvOutNorm adds sum g^2 (FP64, one atomic per block) into *sums; kTvOutUpdate writes
 // o = f - alpha g / sqrt(*sums + 1e-7) (GD_TV.cu:556-597); kTvOutGrad writes o = g.
-template <int OUT>
-__global__ void __launch_bounds__(256) tv_tiled_kernel(const float* __restrict__ f, float* __restrict__ o, TVDims d,
+// ROWS: tile rows per thread; the tile is 32 x (8 ROWS) columns.
+template <int OUT, int ROWS>
+__global__ void __launch_bounds__(256, ROWS == 1 ? 4 : 3) tv_tiled_kernel(const float* __restrict__ f, float* __restrict__ o, TVDims d,
                                                        TvTiles T, double* __restrict__ sums, float alpha) {
-    constexpr int FS = kTvFY * kTvFX;   // one staged slice
+    constexpr int TY = 8 * ROWS, FY = TY + 2, QY = TY + 1;
+    constexpr int FS = FY * kTvFX;            // one staged slice
+    constexpr int NS = (FS + 255) / 256;      // staged elements per thread and slice
     __shared__ float F[3 * FS];
-    // dy, dx and r of a staged slice (dz is needed only at a thread's own column: registers)
-    __shared__ float Qy[2][kTvQY][kTvQX], Qx[2][kTvQY][kTvQX], Qr[2][kTvQY][kTvQX];
+    // dy, dx and r of a staged slice (dz is needed only at a thread's own columns: registers)
+    __shared__ float Qy[2][QY][kTvQX], Qx[2][QY][kTvQX], Qr[2][QY][kTvQX];
     const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5;
     float scale = 0.f;
     if (OUT == kTvOutUpdate) scale = (float)((double)alpha / sqrt(*sums + 1e-7));
     const int plane = d.nx * d.ny;   // the host keeps nx * ny * nz below 2^31
-    // the +x column (qx = 32, qy = 0..8) and the +y row (qy = 8) of difference points
-    const bool extra = tid < kTvQY + kTvTX;
-    const int eqx = tid < kTvQY ? kTvTX : tid - kTvQY, eqy = tid < kTvQY ? tid : kTvTY;
+    // the +x column (qx = 32, qy = 0..TY) and the +y row (qy = TY) of difference points
+    const bool extra = tid < QY + kTvTX;
+    const int eqx = tid < QY ? kTvTX : tid - QY, eqy = tid < QY ? tid : TY;
     double acc = 0.0;
     for (int t = blockIdx.x; t < T.ntiles; t += gridDim.x) {
         const int bx = t % T.tx, rt = t / T.tx;
         const int by = rt % T.ty, bz = rt / T.ty;
-        const int x0 = bx * kTvTX, y0 = by * kTvTY, z0 = bz * kTvZC;
+        const int x0 = bx * kTvTX, y0 = by * TY, z0 = bz * kTvZC;
         const int zend = min(z0 + kTvZC, d.nz);   // output slices z0 .. zend-1; slice zend supplies dz(z+1)
-        // thread tid stages elements k = tid and k = tid + 256 (k < 340) of every slice; their
-        // in-slice offsets are fixed per tile (-1 outside the volume: zero)
-        int off[2];
+        // thread tid stages elements k = tid + 256 j (k < FS) of every slice; their in-slice
+        // offsets are fixed per tile (-1 outside the volume: zero)
+        int off[NS];
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
+        for (int j = 0; j < NS; ++j) {
             const int k = tid + 256 * j;
             const int fy = k / kTvFX, fx = k - fy * kTvFX;
             const int xx = x0 - 1 + fx, yy = y0 - 1 + fy;
             off[j] = (k < FS && xx >= 0 && xx < d.nx && yy >= 0 && yy < d.ny) ? yy * d.nx + xx : -1;
         }
-        auto fetch = [&](int zz, float (&v)[2]) {
+        auto fetch = [&](int zz, float (&v)[NS]) {
             const bool zin = zz >= 0 && zz < d.nz;
 #pragma unroll
-            for (int j = 0; j < 2; ++j) v[j] = (zin && off[j] >= 0) ? __ldg(f + (zz * plane + off[j])) : 0.f;
+            for (int j = 0; j < NS; ++j) v[j] = (zin && off[j] >= 0) ? __ldg(f + (zz * plane + off[j])) : 0.f;
         };
-        auto put = [&](int slot, const float (&v)[2]) {
-            F[slot * FS + tid] = v[0];
-            if (tid + 256 < FS) F[slot * FS + tid + 256] = v[1];
+        auto put = [&](int slot, const float (&v)[NS]) {
+#pragma unroll
+            for (int j = 0; j < NS; ++j)
+                if (j + 1 < NS || tid + 256 * j < FS) F[slot * FS + tid + 256 * j] = v[j];
         };
         // differences and reciprocal norm at point (qx, qy) of slice slot sc over slice slot sp
         auto qpoint = [&](int qx, int qy, int sc, int sp, float& dz, float& dy, float& dx) {
@@ -155,12 +167,18 @@ __global__ void __launch_bounds__(256) tv_tiled_kernel(const float* __restrict__
             dx = x0 + qx > 0 ? c - F[sc * FS + k - 1] : 0.f;
             return tv_rnorm(dz * dz + dy * dy + dx * dx);
         };
-        const int x = x0 + lx, y = y0 + ly;
-        const bool inside = x < d.nx && y < d.ny;
-        const int own = y * d.nx + x;
+        const int x = x0 + lx;
+        bool inside[ROWS];
+        int own[ROWS];
+#pragma unroll
+        for (int q = 0; q < ROWS; ++q) {
+            const int y = y0 + ly + 8 * q;
+            inside[q] = x < d.nx && y < d.ny;
+            own[q] = y * d.nx + x;
+        }
         // R[j]: registers holding a fetched slice; at relative step j the slice zz + 1 is in
         // R[(j + 1) % 3] and slice zz + 3 is fetched into R[j % 3]
-        float R[3][2];
+        float R[3][NS];
         fetch(z0 - 1, R[0]);
         put(0, R[0]);
         fetch(z0, R[0]);
@@ -168,42 +186,52 @@ __global__ void __launch_bounds__(256) tv_tiled_kernel(const float* __restrict__
         fetch(z0 + 1, R[1]);
         fetch(z0 + 2, R[2]);
         __syncthreads();
-        float part = 0.f, fown = 0.f;
+        float part[ROWS], fown[ROWS];
+#pragma unroll
+        for (int q = 0; q < ROWS; ++q) part[q] = fown[q] = 0.f;
         // one slice: slots (SP, SC, SN) hold slices zz - 1, zz, zz + 1; QB is the difference buffer
         auto step = [&](int zz, auto SPc, auto SCc, auto SNc, auto QBc, auto RPc) {
             constexpr int SP = decltype(SPc)::value, SC = decltype(SCc)::value, SN = decltype(SNc)::value;
             constexpr int QB = decltype(QBc)::value, RP = decltype(RPc)::value;
             if (zz + 1 <= zend) put(SN, R[RP]);
             if (zz + 3 <= zend) fetch(zz + 3, R[(RP + 2) % 3]);
-            float dz, dy, dx;
-            const float r = qpoint(lx, ly, SC, SP, dz, dy, dx);
-            Qy[QB][ly][lx] = dy; Qx[QB][ly][lx] = dx; Qr[QB][ly][lx] = r;
+            float dz[ROWS], r[ROWS], dy[ROWS], dx[ROWS];
+#pragma unroll
+            for (int q = 0; q < ROWS; ++q) {
+                const int qy = ly + 8 * q;
+                r[q] = qpoint(lx, qy, SC, SP, dz[q], dy[q], dx[q]);
+                Qy[QB][qy][lx] = dy[q]; Qx[QB][qy][lx] = dx[q]; Qr[QB][qy][lx] = r[q];
+            }
             if (extra) {
                 float a, b, c;
                 const float m = qpoint(eqx, eqy, SC, SP, a, b, c);
                 Qy[QB][eqy][eqx] = b; Qx[QB][eqy][eqx] = c; Qr[QB][eqy][eqx] = m;
             }
             __syncthreads();
-            if (zz > z0 && inside) {   // slice zz-1 is complete with its +z neighbour's term
-                const float g = part - dz * r;
-                if (OUT == kTvOutNorm) acc += (double)g * (double)g;
-                else {
-                    const int i = (zz - 1) * plane + own;
-                    o[i] = OUT == kTvOutUpdate ? fmaf(-scale, g, fown) : g;
+#pragma unroll
+            for (int q = 0; q < ROWS; ++q) {
+                const int qy = ly + 8 * q;
+                if (zz > z0 && inside[q]) {   // slice zz-1 is complete with its +z neighbour's term
+                    const float g = part[q] - dz[q] * r[q];
+                    if (OUT == kTvOutNorm) acc += (double)g * (double)g;
+                    else {
+                        const int i = (zz - 1) * plane + own[q];
+                        o[i] = OUT == kTvOutUpdate ? fmaf(-scale, g, fown[q]) : g;
+                    }
                 }
-            }
-            if (zz < zend && inside) {
-                float g = (dz + dy + dx) * r;
-                if (x + 1 < d.nx) g -= Qx[QB][ly][lx + 1] * Qr[QB][ly][lx + 1];
-                if (y + 1 < d.ny) g -= Qy[QB][ly + 1][lx] * Qr[QB][ly + 1][lx];
-                part = g;
-                fown = F[SC * FS + (ly + 1) * kTvFX + lx + 1];
+                if (zz < zend && inside[q]) {
+                    float g = (dz[q] + dy[q] + dx[q]) * r[q];
+                    if (x + 1 < d.nx) g -= Qx[QB][qy][lx + 1] * Qr[QB][qy][lx + 1];
+                    if (y0 + qy + 1 < d.ny) g -= Qy[QB][qy + 1][lx] * Qr[QB][qy + 1][lx];
+                    part[q] = g;
+                    fown[q] = F[SC * FS + (qy + 1) * kTvFX + lx + 1];
+                }
             }
         };
         using I0 = std::integral_constant<int, 0>;
         using I1 = std::integral_constant<int, 1>;
         using I2 = std::integral_constant<int, 2>;
-        // six relative steps bring the three slots, two buffers and three register pairs back to
+        // six relative steps bring the three slots, two buffers and three register sets back to
         // their starting assignment
         for (int zb = z0; zb <= zend; zb += 6) {
             step(zb, I0{}, I1{}, I2{}, I0{}, I1{});
@@ -224,6 +252,15 @@ __global__ void __launch_bounds__(256) tv_tiled_kernel(const float* __restrict__
         acc = block_sum(acc);
         if (threadIdx.x == 0) atomicAdd(sums, acc);
     }
+}
+
+// launch one tiled pass with the tile shape of tv_rows()
+template <int OUT>
+void launch_tv_tiled(const float* f, float* o, const TVDims& d, double* sums, float alpha, cudaStream_t st) {
+    const int rows = tv_rows();
+    const TvTiles T = tv_tiles(d, rows);
+    if (rows == 2) tv_tiled_kernel<OUT, 2><<<tv_tiled_grid(T), 256, 0, st>>>(f, o, d, T, sums, alpha);
+    else tv_tiled_kernel<OUT, 1><<<tv_tiled_grid(T), 256, 0, st>>>(f, o, d, T, sums, alpha);
 }
 
 // sum_i |grad f_i| over the voxels and the zero halo slice above the last one
@@ -364,9 +401,7 @@ int tigre_tv_gradient(const void* d_img, int dtype, float* d_grad, long nx, long
     if (dtype != TIGRE_F32) return fail(TIGRE_ERR_BAD_ASSERT, "TV kernels take float32 volumes");
     if (nx <= 0 || ny <= 0 || nz <= 0 || !d_img || !d_grad) return fail(TIGRE_ERR_BAD_ASSERT, "bad TV arguments");
     TVDims d{(int)nx, (int)ny, (int)nz};
-    const TvTiles T = tv_tiles(d);
-    tv_tiled_kernel<kTvOutGrad><<<tv_tiled_grid(T), 256, 0, (cudaStream_t)stream>>>((const float*)d_img, d_grad, d, T,
-                                                                                     nullptr, 0.f);
+    launch_tv_tiled<kTvOutGrad>((const float*)d_img, d_grad, d, nullptr, 0.f, (cudaStream_t)stream);
     TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
@@ -396,11 +431,9 @@ int tigre_tv_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha
     TIGRE_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)std::max(max_iter, 1), st));
     float* cur = (float*)d_img;
     float* nxt = d_work;
-    const TvTiles T = tv_tiles(d);
-    const int grid = tv_tiled_grid(T);
     for (int it = 0; it < max_iter; ++it) {
-        tv_tiled_kernel<kTvOutNorm><<<grid, 256, 0, st>>>(cur, nullptr, d, T, sums + it, 0.f);
-        tv_tiled_kernel<kTvOutUpdate><<<grid, 256, 0, st>>>(cur, nxt, d, T, sums + it, alpha);
+        launch_tv_tiled<kTvOutNorm>(cur, nullptr, d, sums + it, 0.f, st);
+        launch_tv_tiled<kTvOutUpdate>(cur, nxt, d, sums + it, alpha, st);
         std::swap(cur, nxt);
     }
     if (cur != (float*)d_img) TIGRE_CUDA(cudaMemcpyAsync(d_img, cur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
@@ -523,11 +556,9 @@ extern "C" int tigre_tv_pocs_noalloc(void* d_img, int dtype, long nx, long ny, l
     if (max_iter > 0) TIGRE_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * (size_t)max_iter, st));
     float* cur = (float*)d_img;
     float* nxt = d_work;
-    const TvTiles T = tv_tiles(d);
-    const int grid = tv_tiled_grid(T);
     for (int it = 0; it < max_iter; ++it) {
-        tv_tiled_kernel<kTvOutNorm><<<grid, 256, 0, st>>>(cur, nullptr, d, T, sums + it, 0.f);
-        tv_tiled_kernel<kTvOutUpdate><<<grid, 256, 0, st>>>(cur, nxt, d, T, sums + it, alpha);
+        launch_tv_tiled<kTvOutNorm>(cur, nullptr, d, sums + it, 0.f, st);
+        launch_tv_tiled<kTvOutUpdate>(cur, nxt, d, sums + it, alpha, st);
         std::swap(cur, nxt);
     }
     if (cur != (float*)d_img) TIGRE_CUDA(cudaMemcpyAsync(d_img, cur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
