@@ -65,22 +65,37 @@ __device__ __forceinline__ double block_sum(double v) {
     return v;
 }
 
-// ---- tiled gradientTV: the POCS passes and the autograd gradient ----
+struct TVStep {
+    const float* prior;   // PICCS prior image (same layout as f)
+    float inv_delta;      // AwTV: 1 / delta
+    float ratio;          // PICCS: weight of the prior term
+    double norm_eps;      // added to sum(g^2) before the square root
+    float grad_eps;       // added to every gradient norm: 1e-8 (GD_AwTV.cu:131), 1e-6 (PICCS.cu:149)
+};
+
+constexpr int kTvPocs = 0, kTvAw = 1, kTvPiccs = 2;
+
+// ---- tiled gradientTV: POCS-TV, AwTV and PICCS passes and the autograd gradient ----
 //
-// A block owns a 32 x 8 tile of (x, y) columns and marches down a chunk of kTvZC slices.
-// Per slice it stages f with a one-voxel x/y halo in shared memory and computes, at every
-// tile point and at the tile's +x column and +y row, the backward differences (dz, dy, dx)
-// and r = 1 / (sqrt(dz^2 + dy^2 + dx^2) + 1e-8) of gradientTV (GD_TV.cu:117-143).  The
-// gradient at (x, y, z) (dftv, GD_TV.cu:135-140) is then
-//     (dz + dy + dx) r  -  dx(x+1) r(x+1)  -  dy(y+1) r(y+1)  -  dz(z+1) r(z+1),
-// with each norm evaluated once instead of four times and each voxel read from global memory
-// once per slice (plus the halo), with no integer division per voxel.  The differences are
-// the reference's exactly; r uses the hardware reciprocal square root and reciprocal, so each
-// term carries a relative error of a few 1e-7 against the reference's IEEE divisions.
-// Zero-filled staging reproduces the boundary rule: the zero slices below z = 0 and above
-// z = nz - 1, and zero differences across the -x / -y faces.
+// A block owns a 32 x (8 ROWS) tile of (x, y) columns and marches down a chunk of kTvZC
+// slices.  Per slice it stages f with a one-voxel x/y halo in shared memory and computes, at
+// every tile point and at the tile's +x column and +y row, the backward differences
+// (dz, dy, dx), their weighted forms (nz, ny, nx) and r = 1 / (sqrt(nz dz + ny dy + nx dx) + eps)
+// -- unweighted for POCS-TV (gradientTV, GD_TV.cu:117-143), with w = exp(-(d / delta)^2) per
+// component for AwTV (GD_AwTV.cu:117-158).  The gradient at (x, y, z) (dftv, GD_TV.cu:135-140)
+// is then
+//     (nz + ny + nx) r  -  nx(x+1) r(x+1)  -  ny(y+1) r(y+1)  -  nz(z+1) r(z+1),
+// each norm and weight evaluated once per voxel instead of four times, each voxel read from
+// global memory once per slice (plus the halo), and no integer division per voxel.  The
+// differences are the reference's exactly; r uses the hardware reciprocal square root and
+// reciprocal, so each term carries a relative error of a few 1e-7 against the reference's
+// IEEE divisions.  Zero-filled staging reproduces the boundary rules: the zero slices below
+// z = 0 and above z = nz - 1 (POCS-TV, AwTV), zero differences across the -x / -y faces.
+// PICCS (PICCS.cu:117-154) runs on the bare image (no z difference at z = 0, no +z term at the
+// last slice, eps 1e-6) and stages two fields, f and f - prior, for
+// g = (1 - ratio) grad TV(f) + ratio grad TV(f - prior).
 //
-// Pipeline: staged slices live in a ring of three buffers and the (dy, dx, r) planes in two,
+// Pipeline: staged slices live in a ring of three buffers and the (ny, nx, r) planes in two,
 // so one barrier per slice suffices; each thread fetches its staged elements three slices
 // ahead into registers, so global loads overlap the arithmetic of the slices before them.
 constexpr int kTvTX = 32, kTvZC = 32;   // tile width; slices per chunk (tile height: 8 rows per thread row)
@@ -101,33 +116,40 @@ TvTiles tv_tiles(const TVDims& d, int rows) {
 
 int tv_tiled_grid(const TvTiles& t) { return std::min(t.ntiles, 148 * 8); }
 
-// rows of the tile each thread owns (1: 32 x 8 tiles, 2: 32 x 16); TIGRE_B200_TV_ROWS overrides
-int tv_rows() {
+// rows of the tile each thread owns (1: 32 x 8 tiles, 2: 32 x 16); TIGRE_B200_TV_ROWS overrides.
+// PICCS, with two staged fields, always uses one row.
+int tv_rows(int kind) {
+    if (kind == kTvPiccs) return 1;
     const char* e = std::getenv("TIGRE_B200_TV_ROWS");
-    return (e && std::atoi(e) == 1) ? 1 : (e && std::atoi(e) == 2) ? 2 : 2;
+    return (e && std::atoi(e) == 1) ? 1 : 2;
 }
 
 // 1 / (sqrt(s) + eps) for s >= 0
-__device__ __forceinline__ float tv_rnorm(float s) {
+__device__ __forceinline__ float tv_rnorm(float s, float eps) {
     const float q = s > 0.f ? s * rsqrtf(s) : 0.f;
-    return __fdividef(1.f, q + 1e-8f);
+    return __fdividef(1.f, q + eps);
 }
 
 // OUT: kTvOutNorm adds sum g^2 (FP64, one atomic per block) into *sums; kTvOutUpdate writes
-// o = f - alpha g / sqrt(*sums + 1e-7) (GD_TV.cu:556-597); kTvOutGrad writes o = g.
-// ROWS: tile rows per thread; the tile is 32 x (8 ROWS) columns.
-template <int OUT, int ROWS>
-__global__ void __launch_bounds__(256, ROWS == 1 ? 4 : 3) tv_tiled_kernel(const float* __restrict__ f, float* __restrict__ o, TVDims d,
-                                                       TvTiles T, double* __restrict__ sums, float alpha) {
+// o = f - alpha g / sqrt(*sums + st.norm_eps) (GD_TV.cu:556-597); kTvOutGrad writes o = g.
+// ROWS: tile rows per thread.  KIND: kTvPocs, kTvAw or kTvPiccs.
+template <int OUT, int ROWS, int KIND>
+__global__ void __launch_bounds__(256, ROWS == 1 ? 4 : 3) tv_tiled_kernel(const float* __restrict__ f,
+                                                                           float* __restrict__ o, TVDims d, TvTiles T,
+                                                                           TVStep st, double* __restrict__ sums,
+                                                                           float alpha) {
+    constexpr bool HALO = KIND != kTvPiccs;
+    constexpr int NF = KIND == kTvPiccs ? 2 : 1;   // staged fields: f (and f - prior)
     constexpr int TY = 8 * ROWS, FY = TY + 2, QY = TY + 1;
-    constexpr int FS = FY * kTvFX;            // one staged slice
-    constexpr int NS = (FS + 255) / 256;      // staged elements per thread and slice
-    __shared__ float F[3 * FS];
-    // dy, dx and r of a staged slice (dz is needed only at a thread's own columns: registers)
-    __shared__ float Qy[2][QY][kTvQX], Qx[2][QY][kTvQX], Qr[2][QY][kTvQX];
+    constexpr int FS = FY * kTvFX;            // one staged slice of one field
+    constexpr int NS = (FS + 255) / 256;      // staged elements per thread, slice and field
+    __shared__ float F[NF * 3 * FS];
+    // ny, nx and r of a staged slice (nz is needed only at a thread's own columns: registers)
+    __shared__ float Qy[NF][2][QY][kTvQX], Qx[NF][2][QY][kTvQX], Qr[NF][2][QY][kTvQX];
     const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5;
+    const float eps = st.grad_eps, idl = st.inv_delta;
     float scale = 0.f;
-    if (OUT == kTvOutUpdate) scale = (float)((double)alpha / sqrt(*sums + 1e-7));
+    if (OUT == kTvOutUpdate) scale = (float)((double)alpha / sqrt(*sums + st.norm_eps));
     const int plane = d.nx * d.ny;   // the host keeps nx * ny * nz below 2^31
     // the +x column (qx = 32, qy = 0..TY) and the +y row (qy = TY) of difference points
     const bool extra = tid < QY + kTvTX;
@@ -137,7 +159,7 @@ __global__ void __launch_bounds__(256, ROWS == 1 ? 4 : 3) tv_tiled_kernel(const 
         const int bx = t % T.tx, rt = t / T.tx;
         const int by = rt % T.ty, bz = rt / T.ty;
         const int x0 = bx * kTvTX, y0 = by * TY, z0 = bz * kTvZC;
-        const int zend = min(z0 + kTvZC, d.nz);   // output slices z0 .. zend-1; slice zend supplies dz(z+1)
+        const int zend = min(z0 + kTvZC, d.nz);   // output slices z0 .. zend-1; slice zend supplies the +z term
         // thread tid stages elements k = tid + 256 j (k < FS) of every slice; their in-slice
         // offsets are fixed per tile (-1 outside the volume: zero)
         int off[NS];
@@ -148,24 +170,41 @@ __global__ void __launch_bounds__(256, ROWS == 1 ? 4 : 3) tv_tiled_kernel(const 
             const int xx = x0 - 1 + fx, yy = y0 - 1 + fy;
             off[j] = (k < FS && xx >= 0 && xx < d.nx && yy >= 0 && yy < d.ny) ? yy * d.nx + xx : -1;
         }
-        auto fetch = [&](int zz, float (&v)[NS]) {
+        auto fetch = [&](int zz, float (&v)[NF][NS]) {
             const bool zin = zz >= 0 && zz < d.nz;
 #pragma unroll
-            for (int j = 0; j < NS; ++j) v[j] = (zin && off[j] >= 0) ? __ldg(f + (zz * plane + off[j])) : 0.f;
+            for (int j = 0; j < NS; ++j) {
+                const bool ok = zin && off[j] >= 0;
+                const int i = zz * plane + off[j];
+                v[0][j] = ok ? __ldg(f + i) : 0.f;
+                if (NF == 2) v[NF - 1][j] = ok ? __ldg(f + i) - __ldg(st.prior + i) : 0.f;
+            }
         };
-        auto put = [&](int slot, const float (&v)[NS]) {
+        auto put = [&](int slot, const float (&v)[NF][NS]) {
 #pragma unroll
-            for (int j = 0; j < NS; ++j)
-                if (j + 1 < NS || tid + 256 * j < FS) F[slot * FS + tid + 256 * j] = v[j];
+            for (int c = 0; c < NF; ++c)
+#pragma unroll
+                for (int j = 0; j < NS; ++j)
+                    if (j + 1 < NS || tid + 256 * j < FS) F[(c * 3 + slot) * FS + tid + 256 * j] = v[c][j];
         };
-        // differences and reciprocal norm at point (qx, qy) of slice slot sc over slice slot sp
-        auto qpoint = [&](int qx, int qy, int sc, int sp, float& dz, float& dy, float& dx) {
+        // weighted differences and reciprocal norm at point (qx, qy) of field c, slice slot sc
+        // over slot sp; zlow: the slice has a z difference (always with the zero halo slices)
+        auto qpoint = [&](int c, int qx, int qy, int sc, int sp, bool zlow, float& wz, float& wy, float& wx) {
             const int k = (qy + 1) * kTvFX + qx + 1;
-            const float c = F[sc * FS + k];
-            dz = c - F[sp * FS + k];
-            dy = y0 + qy > 0 ? c - F[sc * FS + k - kTvFX] : 0.f;
-            dx = x0 + qx > 0 ? c - F[sc * FS + k - 1] : 0.f;
-            return tv_rnorm(dz * dz + dy * dy + dx * dx);
+            const float* Fc = F + (c * 3 + sc) * FS;
+            const float v = Fc[k];
+            const float dz = zlow ? v - F[(c * 3 + sp) * FS + k] : 0.f;
+            const float dy = y0 + qy > 0 ? v - Fc[k - kTvFX] : 0.f;
+            const float dx = x0 + qx > 0 ? v - Fc[k - 1] : 0.f;
+            if (KIND == kTvAw) {
+                const float tz = dz * idl, ty = dy * idl, tx = dx * idl;
+                wz = expf(-(tz * tz)) * dz;
+                wy = expf(-(ty * ty)) * dy;
+                wx = expf(-(tx * tx)) * dx;
+            } else {
+                wz = dz; wy = dy; wx = dx;
+            }
+            return tv_rnorm(wz * dz + wy * dy + wx * dx, eps);
         };
         const int x = x0 + lx;
         bool inside[ROWS];
@@ -178,7 +217,7 @@ __global__ void __launch_bounds__(256, ROWS == 1 ? 4 : 3) tv_tiled_kernel(const 
         }
         // R[j]: registers holding a fetched slice; at relative step j the slice zz + 1 is in
         // R[(j + 1) % 3] and slice zz + 3 is fetched into R[j % 3]
-        float R[3][NS];
+        float R[3][NF][NS];
         fetch(z0 - 1, R[0]);
         put(0, R[0]);
         fetch(z0, R[0]);
@@ -186,33 +225,46 @@ __global__ void __launch_bounds__(256, ROWS == 1 ? 4 : 3) tv_tiled_kernel(const 
         fetch(z0 + 1, R[1]);
         fetch(z0 + 2, R[2]);
         __syncthreads();
-        float part[ROWS], fown[ROWS];
+        float part[NF][ROWS], fown[ROWS];
 #pragma unroll
-        for (int q = 0; q < ROWS; ++q) part[q] = fown[q] = 0.f;
+        for (int q = 0; q < ROWS; ++q) {
+            fown[q] = 0.f;
+#pragma unroll
+            for (int c = 0; c < NF; ++c) part[c][q] = 0.f;
+        }
         // one slice: slots (SP, SC, SN) hold slices zz - 1, zz, zz + 1; QB is the difference buffer
         auto step = [&](int zz, auto SPc, auto SCc, auto SNc, auto QBc, auto RPc) {
             constexpr int SP = decltype(SPc)::value, SC = decltype(SCc)::value, SN = decltype(SNc)::value;
             constexpr int QB = decltype(QBc)::value, RP = decltype(RPc)::value;
             if (zz + 1 <= zend) put(SN, R[RP]);
             if (zz + 3 <= zend) fetch(zz + 3, R[(RP + 2) % 3]);
-            float dz[ROWS], r[ROWS], dy[ROWS], dx[ROWS];
+            const bool zlow = HALO || zz > 0;
+            float wz[NF][ROWS], r[NF][ROWS], wy[NF][ROWS], wx[NF][ROWS];
 #pragma unroll
-            for (int q = 0; q < ROWS; ++q) {
-                const int qy = ly + 8 * q;
-                r[q] = qpoint(lx, qy, SC, SP, dz[q], dy[q], dx[q]);
-                Qy[QB][qy][lx] = dy[q]; Qx[QB][qy][lx] = dx[q]; Qr[QB][qy][lx] = r[q];
-            }
-            if (extra) {
-                float a, b, c;
-                const float m = qpoint(eqx, eqy, SC, SP, a, b, c);
-                Qy[QB][eqy][eqx] = b; Qx[QB][eqy][eqx] = c; Qr[QB][eqy][eqx] = m;
+            for (int c = 0; c < NF; ++c) {
+#pragma unroll
+                for (int q = 0; q < ROWS; ++q) {
+                    const int qy = ly + 8 * q;
+                    r[c][q] = qpoint(c, lx, qy, SC, SP, zlow, wz[c][q], wy[c][q], wx[c][q]);
+                    Qy[c][QB][qy][lx] = wy[c][q]; Qx[c][QB][qy][lx] = wx[c][q]; Qr[c][QB][qy][lx] = r[c][q];
+                }
+                if (extra) {
+                    float a, b, e;
+                    const float m = qpoint(c, eqx, eqy, SC, SP, zlow, a, b, e);
+                    Qy[c][QB][eqy][eqx] = b; Qx[c][QB][eqy][eqx] = e; Qr[c][QB][eqy][eqx] = m;
+                }
             }
             __syncthreads();
+            // without the halo there is no +z neighbour above the last slice
+            const bool zterm = HALO || zz < d.nz;
 #pragma unroll
             for (int q = 0; q < ROWS; ++q) {
                 const int qy = ly + 8 * q;
                 if (zz > z0 && inside[q]) {   // slice zz-1 is complete with its +z neighbour's term
-                    const float g = part[q] - dz[q] * r[q];
+                    float gc[NF];
+#pragma unroll
+                    for (int c = 0; c < NF; ++c) gc[c] = zterm ? part[c][q] - wz[c][q] * r[c][q] : part[c][q];
+                    const float g = NF == 2 ? fmaf(1.f - st.ratio, gc[0], st.ratio * gc[NF - 1]) : gc[0];
                     if (OUT == kTvOutNorm) acc += (double)g * (double)g;
                     else {
                         const int i = (zz - 1) * plane + own[q];
@@ -220,10 +272,13 @@ __global__ void __launch_bounds__(256, ROWS == 1 ? 4 : 3) tv_tiled_kernel(const 
                     }
                 }
                 if (zz < zend && inside[q]) {
-                    float g = (dz[q] + dy[q] + dx[q]) * r[q];
-                    if (x + 1 < d.nx) g -= Qx[QB][qy][lx + 1] * Qr[QB][qy][lx + 1];
-                    if (y0 + qy + 1 < d.ny) g -= Qy[QB][qy + 1][lx] * Qr[QB][qy + 1][lx];
-                    part[q] = g;
+#pragma unroll
+                    for (int c = 0; c < NF; ++c) {
+                        float g = (wz[c][q] + wy[c][q] + wx[c][q]) * r[c][q];
+                        if (x + 1 < d.nx) g -= Qx[c][QB][qy][lx + 1] * Qr[c][QB][qy][lx + 1];
+                        if (y0 + qy + 1 < d.ny) g -= Qy[c][QB][qy + 1][lx] * Qr[c][QB][qy + 1][lx];
+                        part[c][q] = g;
+                    }
                     fown[q] = F[SC * FS + (qy + 1) * kTvFX + lx + 1];
                 }
             }
@@ -254,14 +309,23 @@ __global__ void __launch_bounds__(256, ROWS == 1 ? 4 : 3) tv_tiled_kernel(const 
     }
 }
 
-// launch one tiled pass with the tile shape of tv_rows()
-template <int OUT>
-void launch_tv_tiled(const float* f, float* o, const TVDims& d, double* sums, float alpha, cudaStream_t st) {
-    const int rows = tv_rows();
+// launch one tiled pass with the tile shape of tv_rows(KIND)
+template <int OUT, int KIND>
+void launch_tv_tiled(const float* f, float* o, const TVDims& d, const TVStep& st, double* sums, float alpha,
+                     cudaStream_t s) {
+    const int rows = tv_rows(KIND);
     const TvTiles T = tv_tiles(d, rows);
-    if (rows == 2) tv_tiled_kernel<OUT, 2><<<tv_tiled_grid(T), 256, 0, st>>>(f, o, d, T, sums, alpha);
-    else tv_tiled_kernel<OUT, 1><<<tv_tiled_grid(T), 256, 0, st>>>(f, o, d, T, sums, alpha);
+    if constexpr (KIND != kTvPiccs) {
+        if (rows == 2) {
+            tv_tiled_kernel<OUT, 2, KIND><<<tv_tiled_grid(T), 256, 0, s>>>(f, o, d, T, st, sums, alpha);
+            return;
+        }
+    }
+    tv_tiled_kernel<OUT, 1, KIND><<<tv_tiled_grid(T), 256, 0, s>>>(f, o, d, T, st, sums, alpha);
 }
+
+// POCS-TV step parameters (GD_TV.cu): no prior, no weights, 1e-7 under the norm, 1e-8 per gradient
+constexpr TVStep kPocsStep{nullptr, 0.f, 0.f, 1e-7, 1e-8f};
 
 // sum_i |grad f_i| over the voxels and the zero halo slice above the last one
 // (whose gradient norm is |f(x,y,nz-1)|); its derivative is the gradient of tv_tiled_kernel.
@@ -284,112 +348,6 @@ __global__ void __launch_bounds__(256) tv_value_kernel(const float* __restrict__
     if (threadIdx.x == 0) atomicAdd(out, s);
 }
 
-// ---- adaptive-weighted TV (aw_pocs_tv) and PICCS (piccs_tv) ----
-//
-// Both reuse the backward-difference stencil of gradientTV with two changes:
-// * AwTV (GD_AwTV.cu:117-158): every difference component d_c carries the weight
-//   w_c = exp(-(d_c / delta)^2), in the numerators and inside the norms;
-// * PICCS (PICCS.cu:117-154, :274-380) runs on the bare image (no halo slices: a z
-//   difference whose neighbour is outside is 0, like x and y) and descends along
-//   (1 - ratio) grad TV(f) + ratio grad TV(f - prior), with 1e-6 (not 1e-8) added to each norm.
-// A step is again two passes (norm, then update), with the gradient recomputed.
-
-struct TVStep {
-    const float* prior;   // PICCS prior image (same layout as f)
-    float inv_delta;      // AwTV: 1 / delta
-    float ratio;          // PICCS: weight of the prior term
-    double norm_eps;      // added to sum(g^2) before the square root
-    float grad_eps;       // added to every gradient norm: 1e-8 (GD_AwTV.cu:131), 1e-6 (PICCS.cu:149)
-};
-
-template <bool HALO, bool AW, typename Rd>
-__device__ __forceinline__ float tv_stencil(const Rd& rd, const TVDims& d, int x, int y, int z, float idl, float eps) {
-    auto val = [&](int xx, int yy, int zz) -> float { return (zz >= 0 && zz < d.nz) ? rd(xx, yy, zz) : 0.f; };
-    auto wt = [&](float v) -> float {
-        if (!AW) return 1.f;
-        const float t = v * idl;
-        return expf(-(t * t));
-    };
-    // |grad| with weights: sqrt(w0 a0^2 + w1 a1^2 + w2 a2^2) + eps
-    auto nrm = [&](float a0, float a1, float a2, float w0, float w1, float w2) {
-        return sqrtf(w0 * a0 * a0 + w1 * a1 * a1 + w2 * a2 * a2) + eps;
-    };
-    const bool zlow = HALO || z > 0;
-    const float c = val(x, y, z);
-    const float d0 = zlow ? c - val(x, y, z - 1) : 0.f;
-    const float d1 = y > 0 ? c - val(x, y - 1, z) : 0.f;
-    const float d2 = x > 0 ? c - val(x - 1, y, z) : 0.f;
-    const float w0 = wt(d0), w1 = wt(d1), w2 = wt(d2);
-    float g = (w0 * d0 + w1 * d1 + w2 * d2) / nrm(d0, d1, d2, w0, w1, w2);
-    if (x + 1 < d.nx) {   // neighbour (x+1): its x difference involves f(x)
-        const float n = val(x + 1, y, z);
-        const float e0 = zlow ? n - val(x + 1, y, z - 1) : 0.f;
-        const float e1 = y > 0 ? n - val(x + 1, y - 1, z) : 0.f;
-        const float e2 = n - c;
-        const float v2 = wt(e2);
-        g -= v2 * e2 / nrm(e0, e1, e2, wt(e0), wt(e1), v2);
-    }
-    if (y + 1 < d.ny) {
-        const float n = val(x, y + 1, z);
-        const float e0 = zlow ? n - val(x, y + 1, z - 1) : 0.f;
-        const float e1 = n - c;
-        const float e2 = x > 0 ? n - val(x - 1, y + 1, z) : 0.f;
-        const float v1 = wt(e1);
-        g -= v1 * e1 / nrm(e0, e1, e2, wt(e0), v1, wt(e2));
-    }
-    if (HALO || z + 1 < d.nz) {   // neighbour (z+1); with the halo, above the last slice it is 0
-        const float n = val(x, y, z + 1);
-        const float e0 = n - c;
-        const float e1 = y > 0 ? n - val(x, y - 1, z + 1) : 0.f;
-        const float e2 = x > 0 ? n - val(x - 1, y, z + 1) : 0.f;
-        const float v0 = wt(e0);
-        g -= v0 * e0 / nrm(e0, e1, e2, v0, wt(e1), wt(e2));
-    }
-    return g;
-}
-
-constexpr int kTvAw = 1, kTvPiccs = 2;
-
-template <int KIND>
-__device__ __forceinline__ float tv_step_grad(const float* __restrict__ f, const TVDims& d, const TVStep& s, int x,
-                                              int y, int z) {
-    auto rf = [&](int xx, int yy, int zz) { return __ldg(f + ((size_t)zz * d.ny + yy) * d.nx + xx); };
-    if (KIND == kTvAw) return tv_stencil<true, true>(rf, d, x, y, z, s.inv_delta, s.grad_eps);
-    auto rdiff = [&](int xx, int yy, int zz) {
-        const size_t i = ((size_t)zz * d.ny + yy) * d.nx + xx;
-        return __ldg(f + i) - __ldg(s.prior + i);
-    };
-    const float ga = tv_stencil<false, false>(rf, d, x, y, z, 0.f, s.grad_eps);
-    const float gb = tv_stencil<false, false>(rdiff, d, x, y, z, 0.f, s.grad_eps);
-    return fmaf(1.f - s.ratio, ga, s.ratio * gb);
-}
-
-template <int KIND>
-__global__ void __launch_bounds__(256) tv_step_norm_kernel(const float* __restrict__ f, TVDims d, TVStep st,
-                                                           double* __restrict__ out) {
-    double s = 0.0;
-    TV_FOR_EACH_VOXEL(d, d.nz, x, y, z, i) {
-        (void)i;
-        const float g = tv_step_grad<KIND>(f, d, st, x, y, z);
-        s += (double)g * (double)g;
-    }
-    TV_END_FOR_EACH_VOXEL
-    s = block_sum(s);
-    if (threadIdx.x == 0) atomicAdd(out, s);
-}
-
-template <int KIND>
-__global__ void __launch_bounds__(256) tv_step_update_kernel(const float* __restrict__ f, float* __restrict__ o,
-                                                             TVDims d, TVStep st, const double* __restrict__ sumsq,
-                                                             float alpha) {
-    const float scale = (float)((double)alpha / sqrt(*sumsq + st.norm_eps));
-    TV_FOR_EACH_VOXEL(d, d.nz, x, y, z, i) {
-        const float g = tv_step_grad<KIND>(f, d, st, x, y, z);
-        o[i] = fmaf(-scale, g, __ldg(f + i));
-    }
-    TV_END_FOR_EACH_VOXEL
-}
-
 }  // namespace
 }  // namespace tigre
 
@@ -401,7 +359,7 @@ int tigre_tv_gradient(const void* d_img, int dtype, float* d_grad, long nx, long
     if (dtype != TIGRE_F32) return fail(TIGRE_ERR_BAD_ASSERT, "TV kernels take float32 volumes");
     if (nx <= 0 || ny <= 0 || nz <= 0 || !d_img || !d_grad) return fail(TIGRE_ERR_BAD_ASSERT, "bad TV arguments");
     TVDims d{(int)nx, (int)ny, (int)nz};
-    launch_tv_tiled<kTvOutGrad>((const float*)d_img, d_grad, d, nullptr, 0.f, (cudaStream_t)stream);
+    launch_tv_tiled<kTvOutGrad, kTvPocs>((const float*)d_img, d_grad, d, kPocsStep, nullptr, 0.f, (cudaStream_t)stream);
     TIGRE_LAUNCHED();
     return TIGRE_SUCCESS;
 }
@@ -432,8 +390,8 @@ int tigre_tv_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha
     float* cur = (float*)d_img;
     float* nxt = d_work;
     for (int it = 0; it < max_iter; ++it) {
-        launch_tv_tiled<kTvOutNorm>(cur, nullptr, d, sums + it, 0.f, st);
-        launch_tv_tiled<kTvOutUpdate>(cur, nxt, d, sums + it, alpha, st);
+        launch_tv_tiled<kTvOutNorm, kTvPocs>(cur, nullptr, d, kPocsStep, sums + it, 0.f, st);
+        launch_tv_tiled<kTvOutUpdate, kTvPocs>(cur, nxt, d, kPocsStep, sums + it, alpha, st);
         std::swap(cur, nxt);
     }
     if (cur != (float*)d_img) TIGRE_CUDA(cudaMemcpyAsync(d_img, cur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
@@ -457,8 +415,8 @@ static int tv_descent(void* d_img, long nx, long ny, long nz, float alpha, int m
     float* cur = (float*)d_img;
     float* nxt = d_work;
     for (int it = 0; it < max_iter; ++it) {
-        tv_step_norm_kernel<KIND><<<grid_rows(d, d.nz), 256, 0, st>>>(cur, d, stp, sums + it);
-        tv_step_update_kernel<KIND><<<grid_rows(d, d.nz), 256, 0, st>>>(cur, nxt, d, stp, sums + it, alpha);
+        launch_tv_tiled<kTvOutNorm, KIND>(cur, nullptr, d, stp, sums + it, 0.f, st);
+        launch_tv_tiled<kTvOutUpdate, KIND>(cur, nxt, d, stp, sums + it, alpha, st);
         std::swap(cur, nxt);
     }
     if (cur != (float*)d_img) TIGRE_CUDA(cudaMemcpyAsync(d_img, cur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
@@ -557,8 +515,8 @@ extern "C" int tigre_tv_pocs_noalloc(void* d_img, int dtype, long nx, long ny, l
     float* cur = (float*)d_img;
     float* nxt = d_work;
     for (int it = 0; it < max_iter; ++it) {
-        launch_tv_tiled<kTvOutNorm>(cur, nullptr, d, sums + it, 0.f, st);
-        launch_tv_tiled<kTvOutUpdate>(cur, nxt, d, sums + it, alpha, st);
+        launch_tv_tiled<kTvOutNorm, kTvPocs>(cur, nullptr, d, kPocsStep, sums + it, 0.f, st);
+        launch_tv_tiled<kTvOutUpdate, kTvPocs>(cur, nxt, d, kPocsStep, sums + it, alpha, st);
         std::swap(cur, nxt);
     }
     if (cur != (float*)d_img) TIGRE_CUDA(cudaMemcpyAsync(d_img, cur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
