@@ -141,6 +141,37 @@ def cpu_baseline(geo, ang, n_views=4):
             "sample": "FP64 oracle Siddon, %d of %d views, full %dx%d detector, %.1f s" % (n_views, NA, NU, NV, dt)}
 
 
+def cpu_configs(c2_views=36):
+    """The FP64 oracle (all host cores) on the small configurations: C1 (64^3 @ 1 mm, 128x128 @
+    0.8 mm, 100 views) in full, and C2 (256^3 @ 1 mm, 512x512 @ 0.8 mm, 360 views over 2 pi) on
+    c2_views evenly spaced views, rates extrapolated per ray / per voxel update."""
+    from oracle import oracle as O
+    from tigre_b200.utilities.geometry import cone_geometry
+    from tigre_b200.utilities.phantom import random_ellipsoids
+    out = {"impl": "oracle-cpu", "cores": os.cpu_count(), "kind": "port", "configs": {}}
+    for name, n, nd, dd, na, nv in (("C1", 64, 128, 0.8, 100, 100), ("C2", 256, 512, 0.8, 360, c2_views)):
+        geo = cone_geometry((n, n, n), (float(n),) * 3, (nd, nd), (dd, dd))
+        ang = np.linspace(0, 2 * np.pi, na, endpoint=False).astype(np.float32)[
+            np.linspace(0, na, nv, endpoint=False).astype(int)]
+        img = random_ellipsoids((n, n, n), seed=0)
+        rays, upd = nv * nd * nd, nv * n ** 3
+        res = {"views_timed": nv, "views": na}
+        for op, fn, units, unit in (
+                ("ax_siddon", lambda: O.ax(img, geo, ang, "Siddon"), rays, "GRays/s"),
+                ("ax_interpolated", lambda: O.ax(img, geo, ang, "interpolated"), rays, "GRays/s")):
+            t = time.perf_counter()
+            proj = fn()
+            dt = time.perf_counter() - t
+            res[op] = {"value": round(units / dt / 1e9, 6), "unit": unit, "s": round(dt, 3)}
+        for op, kind in (("atb_fdk", "FDK"), ("atb_matched", "matched")):
+            t = time.perf_counter()
+            O.atb(proj, geo, ang, kind)
+            dt = time.perf_counter() - t
+            res[op] = {"value": round(upd / dt / 1e9, 6), "unit": "Gvox-upd/s", "s": round(dt, 3)}
+        out["configs"][name] = res
+    return out
+
+
 _PH = {}
 
 
@@ -223,7 +254,12 @@ def main():
     ap.add_argument("--no-ops", action="store_true", help="skip the per-kind kernel timings")
     ap.add_argument("--size", type=int, default=512, choices=[512, 256])
     ap.add_argument("--views", type=int, default=0)
+    ap.add_argument("--cpu-configs", action="store_true",
+                    help="only time the FP64 CPU oracle on the C1 and C2 configurations and print one JSON line")
     args = ap.parse_args()
+    if args.cpu_configs:
+        print(json.dumps(cpu_configs()))
+        return
     set_size(args.size, args.views)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -369,6 +405,15 @@ def time_ops(P, plan, vol, proj, reps=3):
     tv_vol, tv_work = vol.clone(), torch.empty_like(vol)
     cases["tv_pocs_f32"] = (lambda: P.tv_pocs_(tv_vol, TV_ALPHA, TV_ITERS, tv_work), math.prod(NVOX) * TV_ITERS,
                             "Gvox-iter/s")
+    # algorithmic bytes per launch (FP32 / BF16 element bytes e): interpolated: 8 corner reads per
+    # sample inside the volume + one output write per ray; backprojection: 4 bilinear taps per
+    # voxel update + one volume write; POCS-TV: 12 B per voxel and step (norm pass reads f,
+    # update pass reads f and writes f')
+    nsamp = P.interp_samples(plan)
+    nvox = math.prod(NVOX)
+    alg = {"ax_interpolated_f32": nsamp * 8 * 4 + rays * 4, "ax_interpolated_bf16": nsamp * 8 * 2 + rays * 2,
+           "atb_fdk_f32": upd * 4 * 4 + nvox * 4, "atb_matched_bf16": upd * 4 * 2 + nvox * 2,
+           "atb_fdk_bf16": upd * 4 * 2 + nvox * 2, "tv_pocs_f32": nvox * 12 * TV_ITERS}
     out = {}
     for name, (fn, units, unit) in cases.items():
         fn()
@@ -381,6 +426,11 @@ def time_ops(P, plan, vol, proj, reps=3):
         torch.cuda.synchronize()
         dt = e0.elapsed_time(e1) / 1e3 / reps
         out[name] = {"value": round(units / dt / 1e9, 4), "unit": unit, "ms_per_launch": round(1e3 * dt, 3)}
+        if name in alg:
+            peak = peaks()[0]
+            out[name]["alg_gbs"] = round(alg[name] / dt / 1e9, 1)
+            out[name]["alg_frac_of_hbm"] = round(alg[name] / dt / 1e9 / peak, 4)
+    out["interp_samples"] = nsamp
     del vol16, proj16, p_out, v_out, p16_out, v16_out, tv_vol, tv_work
     # POCS-TV through the host API (numpy in and out, copies included), as minTV is called
     from tigre_b200.utilities.minTV import minTV

@@ -208,6 +208,12 @@ void tigre_release_cache(void);
  * no traversal); the algorithmic-bytes count of the Siddon roofline. */
 int tigre_siddon_count_segments(TigrePlan* plan, int angle_begin, int angle_end, unsigned long long* d_total,
                                 void* stream);
+/* Sum over all rays of the number of interpolated samples strictly inside the volume's open
+ * box (-1, n) per axis, i.e. those whose trilinear footprint can be nonzero (FP64 ray setup of
+ * ray_interpolated_projection.cu:153-199, no sampling); the algorithmic-bytes count of the
+ * interpolated projector's roofline. */
+int tigre_interp_count_samples(TigrePlan* plan, int angle_begin, int angle_end, unsigned long long* d_total,
+                               void* stream);
 
 /* POCS-TV on a device volume, in place: max_iter steps of GD_TV.cu:440-597.
  * d_work: caller scratch of nx*ny*nz floats (same dtype as d_img is not required: FP32). */

@@ -90,6 +90,22 @@ def test_siddon_segment_count_matches_oracle():
     assert abs(total - int(cnt.sum())) <= 1e-4 * int(cnt.sum()), (total, int(cnt.sum()))
 
 
+@pytest.mark.parametrize("tilt", [False, True])
+def test_interp_sample_count_matches_oracle(tilt):
+    """tigre_interp_count_samples against the oracle's per-ray sample counts (samples strictly
+    inside the open box), axial and with theta/psi rotations (the spherical cap)."""
+    _torch()
+    from tigre_b200 import _native as N, projectors
+    geo, ang = G.c1_geometry(), G.angles(20, tilt=tilt)
+    img = G.phantom((64, 64, 64))
+    _, cnt = O.ax(img, geo, ang, "interpolated", return_counts=True)
+    plan = N.get_plan(N.checked_geometry(geo, ang), 0)
+    total = projectors.interp_samples(plan)
+    ref = int(cnt.sum())
+    # boundary samples whose coordinate rounds onto -1 or n may fall either way
+    assert ref > 0 and abs(total - ref) <= 1e-4 * ref, (total, ref)
+
+
 def test_angle_subrange_matches_full():
     torch = _torch()
     from tigre_b200 import _native as N, projectors

@@ -86,6 +86,7 @@ _SIGS = {
                                C.c_int, C.c_void_p]),
     "tigre_release_cache": (None, []),
     "tigre_siddon_count_segments": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "tigre_interp_count_samples": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "tigre_tv_pocs": (C.c_int, [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_int, C.c_void_p,
                                 C.c_void_p]),
     "tigre_tv_pocs_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_int,

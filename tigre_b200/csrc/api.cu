@@ -188,6 +188,13 @@ int tigre_siddon_count_segments(TigrePlan* plan, int a0, int a1, unsigned long l
     return launch_siddon_count(plan, a0, a1, d_total, (cudaStream_t)stream);
 }
 
+int tigre_interp_count_samples(TigrePlan* plan, int a0, int a1, unsigned long long* d_total, void* stream) {
+    if (int rc = check_range(plan, a0, a1)) return rc;
+    if (!d_total) return fail(TIGRE_ERR_BAD_ASSERT, "null output");
+    DeviceGuard g(plan->device);
+    return launch_interp_count(plan, a0, a1, d_total, (cudaStream_t)stream);
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------- host API --

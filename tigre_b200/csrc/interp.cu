@@ -66,8 +66,56 @@ __device__ __forceinline__ float tri(const float4 q0, const float4 q1, float ff,
 
 __device__ __forceinline__ float2 pk2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ float2 pk2(float a) { return make_float2(a, a); }
-__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 t) {
-    return __ffma2_rn(t, __ffma2_rn(a, pk2(-1.f), b), a);
+
+// FP64 ray setup of detector pixel (u, v): source s, step vector vec and the last sample index
+// (the reference's length, capped per view).
+__device__ __forceinline__ double interp_setup(const InterpArgs& p, const FrameInterp& F, int u, int v, double (&s)[3],
+                                               double (&vec)[3]) {
+    const double pv = (double)(p.nV - 1 - v);
+    double d[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        s[k] = p.parallel ? fma(pv, F.dv[k], fma((double)u, F.du[k], F.s[k])) : F.s[k];
+        d[k] = fma(pv, F.dv[k], fma((double)u, F.du[k], F.o[k])) - s[k];
+    }
+    const double len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    double length = ceil(len / p.acc);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) vec[k] = d[k] / length;
+    if (F.cap < length) length = ceil(F.cap);
+    return length;
+}
+
+// Number of samples of each ray strictly inside the open box (-1, n) per axis -- the samples
+// whose trilinear footprint can be nonzero, the count of the oracle's interp_ray -- summed
+// over the launch into *total (the algorithmic-bytes numerator of the interpolated roofline).
+__global__ void __launch_bounds__(256) interp_count_kernel(InterpArgs p, unsigned long long* total) {
+    const int u = blockIdx.x * 32 + threadIdx.x;
+    const int la = blockIdx.y;
+    const int v = blockIdx.z * blockDim.y + threadIdx.y;
+    unsigned long long c = 0;
+    if (u < p.nU && v < p.nV) {
+        const FrameInterp& F = p.frames[p.a0 + la];
+        double s[3], vec[3];
+        const double length = interp_setup(p, F, u, v, s, vec);
+        double lo = F.first_sample, hi = length;
+        const int n[3] = {p.nX, p.nY, p.nZ};
+        bool empty = false;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (vec[k] != 0.0) {
+                const double ta = (-1.0 - s[k]) / vec[k], tb = ((double)n[k] - s[k]) / vec[k];
+                lo = fmax(lo, floor(fmin(ta, tb)) + 1.0);
+                hi = fmin(hi, ceil(fmax(ta, tb)) - 1.0);
+            } else if (s[k] <= -1.0 || s[k] >= (double)n[k]) {
+                empty = true;
+            }
+        }
+        if (!empty && lo <= hi) c = (unsigned long long)(hi - lo + 1.0);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(total, c);
 }
 
 template <typename TV, typename TP, bool NEAREST>
@@ -81,17 +129,8 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs p) {
     const bool in_u = u0 < p.nU;
     const int u = in_u ? u0 : p.nU - 1;
     const FrameInterp& F = p.frames[p.a0 + la];
-    const double pv = (double)(p.nV - 1 - v);
-    double d[3], s[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        s[k] = p.parallel ? fma(pv, F.dv[k], fma((double)u, F.du[k], F.s[k])) : F.s[k];
-        d[k] = fma(pv, F.dv[k], fma((double)u, F.du[k], F.o[k])) - s[k];
-    }
-    const double len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-    double length = ceil(len / p.acc);
-    double vec[3] = {d[0] / length, d[1] / length, d[2] / length};
-    if (F.cap < length) length = ceil(F.cap);
+    double s[3], vec[3];
+    const double length = interp_setup(p, F, u, v, s, vec);
     double lo = F.first_sample, hi = length;
     const int n[3] = {p.nX, p.nY, p.nZ};
     bool empty = false;
@@ -215,6 +254,26 @@ void launch_typed(const InterpArgs& a, bool nearest, dim3 grid, dim3 block, cuda
 }
 
 }  // namespace
+
+int launch_interp_count(TigrePlan* P, int a0, int a1, unsigned long long* d_total, cudaStream_t st) {
+    InterpArgs a{};
+    a.frames = P->d_interp;
+    a.nX = P->d.nX; a.nY = P->d.nY; a.nZ = P->d.nZ; a.nU = P->d.nU; a.nV = P->d.nV;
+    a.dVX = P->d.dVX; a.dVY = P->d.dVY; a.dVZ = P->d.dVZ; a.acc = P->d.accuracy;
+    a.parallel = P->parallel ? 1 : 0;
+    const int rows = 8;
+    dim3 block(32, rows);
+    dim3 grid((P->d.nU + 31) / 32, 1, (P->d.nV + rows - 1) / rows);
+    TIGRE_CUDA(cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), st));
+    for (int c = 0; c < a1 - a0; c += 65535) {
+        InterpArgs ac = a;
+        ac.a0 = a0 + c;
+        grid.y = std::min(65535, a1 - a0 - c);
+        interp_count_kernel<<<grid, block, 0, st>>>(ac, d_total);
+        TIGRE_LAUNCHED();
+    }
+    return TIGRE_SUCCESS;
+}
 
 int launch_interp(TigrePlan* P, const void* vol_x, const void* vol_y, const void* quad_x, const void* quad_y, int vdt,
                   void* proj, int pdt, int a0, int a1, cudaStream_t st) {

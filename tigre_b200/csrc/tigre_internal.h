@@ -155,6 +155,7 @@ int launch_repitch_projections_f32(const void* src, int dtype, float* dst, int n
 int launch_siddon(TigrePlan* p, const void* vol_x, const void* vol_y, int vdt, void* proj, int pdt, int a0, int a1,
                   cudaStream_t st);
 int launch_siddon_count(TigrePlan* p, int a0, int a1, unsigned long long* d_total, cudaStream_t st);
+int launch_interp_count(TigrePlan* p, int a0, int a1, unsigned long long* d_total, cudaStream_t st);
 int launch_siddon_cells(TigrePlan* p, const void* vol_z, int vdt, void* proj, int pdt, int a0, int a1,
                         cudaStream_t st);
 int launch_siddon_columns(TigrePlan* p, const void* vol_z, int vdt, void* proj, int pdt, int a0, int a1,

@@ -93,6 +93,17 @@ def siddon_segments(plan: "N.Plan", angle_range=None, device=None) -> int:
     return int(tot.item())
 
 
+def interp_samples(plan: "N.Plan", angle_range=None) -> int:
+    """Total number of interpolated samples inside the volume over the plan's rays (FP64 setup only)."""
+    a0, a1 = _range(plan, angle_range)
+    dev = torch.device("cuda", plan.device)
+    tot = torch.zeros(1, dtype=torch.int64, device=dev)
+    N.check(N.lib().tigre_interp_count_samples(plan.handle, a0, a1, C.c_void_p(tot.data_ptr()),
+                                               C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)),
+            "tigre_interp_count_samples")
+    return int(tot.item())
+
+
 def _vol3(t: torch.Tensor):
     if t.dim() != 3 or not t.is_cuda or not t.is_contiguous() or t.dtype != torch.float32:
         raise ValueError("expected a contiguous float32 CUDA volume (nZ, nY, nX)")
