@@ -311,9 +311,10 @@ std::vector<DeviceState*> g_states;
 
 // ---- host <-> device copies of pageable memory ----
 // An upload from pageable memory goes through the driver's own small staging buffers at a
-// fraction of the link's bandwidth.  Uploads of at least kStageMin bytes instead go through two
-// pinned bounce buffers of kStageBytes: up to kStageThreads host threads copy chunk k into one
-// while the copy engine moves chunk k - 1 through the other.
+// fraction of the link's bandwidth.  Pageable uploads of at least kStageMin bytes instead go
+// through two pinned bounce buffers of kStageBytes: up to kStageThreads host threads copy chunk
+// k into one while the copy engine moves chunk k - 1 through the other.  Page-locked caller
+// buffers keep the direct path.
 constexpr size_t kStageBytes = (size_t)64 << 20;
 constexpr size_t kStageMin = (size_t)32 << 20;
 constexpr unsigned kStageThreads = 8;
@@ -349,6 +350,17 @@ void par_memcpy(void* dst, const void* src, size_t n) {
     for (auto& th : pool) th.join();
 }
 
+// true when p is page-locked host memory (cudaHostAlloc / cudaHostRegister): the copy engine
+// reads and writes it directly, so a bounce buffer would only add a host copy
+bool host_pinned(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 int ensure_pinned(DeviceState* S) {
     for (auto& p : S->pin)
         if (!p) TIGRE_CUDA(cudaMallocHost(&p, kStageBytes));
@@ -357,7 +369,7 @@ int ensure_pinned(DeviceState* S) {
 
 // h_src (pageable) -> d_dst on stream st; returns once h_src may be reused
 int staged_h2d(DeviceState* S, void* d_dst, const void* h_src, size_t n, cudaStream_t st, int which = 1) {
-    if (n < kStageMin || !staging_on(which)) {
+    if (n < kStageMin || !staging_on(which) || host_pinned(h_src)) {
         TIGRE_CUDA(cudaMemcpyAsync(d_dst, h_src, n, cudaMemcpyHostToDevice, st));
         return TIGRE_SUCCESS;
     }
@@ -376,7 +388,7 @@ int staged_h2d(DeviceState* S, void* d_dst, const void* h_src, size_t n, cudaStr
 
 // d_src -> h_dst (pageable) after the work already queued on st; returns when h_dst is written
 int staged_d2h(DeviceState* S, void* h_dst, const void* d_src, size_t n, cudaStream_t st, int which = 2) {
-    if (n < kStageMin || !staging_on(which)) {
+    if (n < kStageMin || !staging_on(which) || host_pinned(h_dst)) {
         TIGRE_CUDA(cudaMemcpyAsync(h_dst, d_src, n, cudaMemcpyDeviceToHost, st));
         TIGRE_CUDA(cudaStreamSynchronize(st));
         return TIGRE_SUCCESS;
