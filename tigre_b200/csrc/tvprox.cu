@@ -13,7 +13,8 @@
 // copy then lands), and both evolve with the rest.
 //
 // Layout here: f, u, px, py, pz as (nZ + 2, nY, nX) x-fastest arrays in one work buffer.
-// Each update is one pass over the volume (one thread per voxel, neighbours through L1);
+// Each update is one pass over the volume (blocks over rows, threads along x, neighbours
+// through L1);
 // a step moves ~52 bytes per voxel, so the operator is HBM bound.
 
 #include <cmath>
@@ -28,29 +29,35 @@ struct ProxDims {
     float idx, idy, idz;     // 1 / spacing
 };
 
+// Voxels of the (nzp, ny, nx) arrays: blocks stride over (y, z) rows, threads over x, so no
+// thread divides a linear index; i is the linear index of (x, y, z).
+#define PROX_FOR_EACH_VOXEL(d, x, y, z, i)                                                   \
+    for (long row_ = blockIdx.x; row_ < (long)(d).ny * (d).nzp; row_ += gridDim.x) {        \
+        const int y = (int)(row_ % (d).ny), z = (int)(row_ / (d).ny);                         \
+        for (int x = threadIdx.x; x < (d).nx; x += blockDim.x) {                               \
+            const long i = row_ * (d).nx + x;
+#define PROX_END_FOR_EACH_VOXEL \
+    }                           \
+    }
+
 __global__ void __launch_bounds__(256) prox_update_u(const float* __restrict__ f, const float* __restrict__ pz,
                                                      const float* __restrict__ py, const float* __restrict__ px,
                                                      float* __restrict__ u, float tau, float inv_lambda, ProxDims d) {
-    const long plane = (long)d.nx * d.ny, n = plane * d.nzp;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        const int x = (int)(i % d.nx);
-        const long r = i / d.nx;
-        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
+    const long plane = (long)d.nx * d.ny;
+    PROX_FOR_EACH_VOXEL(d, x, y, z, i) {
         float div = z > 0 ? (pz[i] - pz[i - plane]) * d.idz : pz[i];
         div += y > 0 ? (py[i] - py[i - d.nx]) * d.idy : py[i];
         div += x > 0 ? (px[i] - px[i - 1]) * d.idx : px[i];
         u[i] = u[i] * (1.f - tau) + tau * (f[i] + inv_lambda * div);
     }
+    PROX_END_FOR_EACH_VOXEL
 }
 
 __global__ void __launch_bounds__(256) prox_update_p(const float* __restrict__ u, float* __restrict__ pz,
                                                      float* __restrict__ py, float* __restrict__ px, float tau,
                                                      ProxDims d) {
-    const long plane = (long)d.nx * d.ny, n = plane * d.nzp;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        const int x = (int)(i % d.nx);
-        const long r = i / d.nx;
-        const int y = (int)(r % d.ny), z = (int)(r / d.ny);
+    const long plane = (long)d.nx * d.ny;
+    PROX_FOR_EACH_VOXEL(d, x, y, z, i) {
         const float c = u[i];
         const float gz = z + 1 < d.nzp ? (u[i + plane] - c) * d.idz : 0.f;
         const float gy = y + 1 < d.ny ? (u[i + d.nx] - c) * d.idy : 0.f;
@@ -61,10 +68,11 @@ __global__ void __launch_bounds__(256) prox_update_p(const float* __restrict__ u
         py[i] = q1 / nrm;
         px[i] = q2 / nrm;
     }
+    PROX_END_FOR_EACH_VOXEL
 }
 
-int grid_for_prox(long n) {
-    return (int)std::min<long>((n + 255) / 256, 148L * 16);
+int grid_for_prox(const ProxDims& d) {
+    return (int)std::min<long>((long)d.ny * d.nzp, 148L * 16);
 }
 
 }  // namespace
@@ -100,7 +108,7 @@ int tigre_tv_denoise(const float* d_src, float* d_dst, long nx, long ny, long nz
     TIGRE_CUDA(cudaMemcpyAsync(u, f, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
     TIGRE_CUDA(cudaMemsetAsync(pz, 0, sizeof(float) * n * 3, st));
     ProxDims d{(int)nx, (int)ny, (int)(nz + 2), 1.f / sx, 1.f / sy, 1.f / sz};
-    const int grid = grid_for_prox(n);
+    const int grid = grid_for_prox(d);
     for (int i = 0; i < max_iter; ++i) {
         const float tau2 = 0.3f + 0.02f * (float)i;
         const float tau1 = (1.f / tau2) * ((1.f / 6.f) - (5.f / (15.f + (float)i)));
