@@ -344,7 +344,12 @@ void par_memcpy(void* dst, const void* src, size_t n) {
     for (unsigned t = 1; t < T; ++t) {
         const size_t a = (size_t)t * per;
         if (a >= n) break;
-        pool.emplace_back([=] { memcpy((char*)dst + a, (const char*)src + a, std::min(per, n - a)); });
+        try {
+            pool.emplace_back([=] { memcpy((char*)dst + a, (const char*)src + a, std::min(per, n - a)); });
+        } catch (...) {   // no thread (resource limits): the calling thread copies the rest
+            memcpy((char*)dst + a, (const char*)src + a, n - a);
+            break;
+        }
     }
     memcpy(dst, src, std::min(per, n));
     for (auto& th : pool) th.join();
