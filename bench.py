@@ -405,6 +405,11 @@ def time_ops(P, plan, vol, proj, reps=3):
     tv_vol, tv_work = vol.clone(), torch.empty_like(vol)
     cases["tv_pocs_f32"] = (lambda: P.tv_pocs_(tv_vol, TV_ALPHA, TV_ITERS, tv_work), math.prod(NVOX) * TV_ITERS,
                             "Gvox-iter/s")
+    tv_prior = (vol * 0.9).contiguous()
+    cases["tv_awtv_f32"] = (lambda: P.tv_aw_pocs_(tv_vol, TV_ALPHA, TV_ITERS, 0.02, tv_work),
+                            math.prod(NVOX) * TV_ITERS, "Gvox-iter/s")
+    cases["tv_piccs_f32"] = (lambda: P.tv_piccs_(tv_vol, tv_prior, TV_ALPHA, 0.5, TV_ITERS, tv_work),
+                             math.prod(NVOX) * TV_ITERS, "Gvox-iter/s")
     from tigre_b200.utilities.im_3d_denoise import tv_denoise_device
     prox_work = torch.empty(5 * NVOX[1] * NVOX[2] * (NVOX[0] + 2), dtype=torch.float32, device=vol.device)
     cases["tv_denoise_f32"] = (lambda: tv_denoise_device(vol, TV_ITERS, 15.0, prox_work), math.prod(NVOX) * TV_ITERS,
@@ -412,14 +417,16 @@ def time_ops(P, plan, vol, proj, reps=3):
     # algorithmic bytes per launch (FP32 / BF16 element bytes e): interpolated: 8 corner reads per
     # sample inside the volume + one output write per ray; backprojection: 4 bilinear taps per
     # voxel update + one volume write; POCS-TV: 12 B per voxel and step (norm pass reads f,
-    # update pass reads f and writes f'); TV proximal: 52 B per voxel and iteration (u pass reads
-    # f, u, p and writes u; p pass reads u, p and writes p)
+    # update pass reads f and writes f'; AwTV the same; PICCS 20 B, the prior read in both passes);
+    # TV proximal: 52 B per voxel and iteration (u pass reads f, u, p and writes u; p pass reads
+    # u, p and writes p)
     nsamp = P.interp_samples(plan)
     nvox = math.prod(NVOX)
     alg = {"ax_interpolated_f32": nsamp * 8 * 4 + rays * 4, "ax_interpolated_bf16": nsamp * 8 * 2 + rays * 2,
            "atb_fdk_f32": upd * 4 * 4 + nvox * 4, "atb_matched_bf16": upd * 4 * 2 + nvox * 2,
            "atb_fdk_bf16": upd * 4 * 2 + nvox * 2, "tv_pocs_f32": nvox * 12 * TV_ITERS,
-           "tv_denoise_f32": nvox * 52 * TV_ITERS}
+           "tv_denoise_f32": nvox * 52 * TV_ITERS, "tv_awtv_f32": nvox * 12 * TV_ITERS,
+           "tv_piccs_f32": nvox * 20 * TV_ITERS}
     out = {}
     for name, (fn, units, unit) in cases.items():
         fn()
@@ -437,7 +444,7 @@ def time_ops(P, plan, vol, proj, reps=3):
             out[name]["alg_gbs"] = round(alg[name] / dt / 1e9, 1)
             out[name]["alg_frac_of_hbm"] = round(alg[name] / dt / 1e9 / peak, 4)
     out["interp_samples"] = nsamp
-    del vol16, proj16, p_out, v_out, p16_out, v16_out, tv_vol, tv_work, prox_work
+    del vol16, proj16, p_out, v_out, p16_out, v16_out, tv_vol, tv_work, prox_work, tv_prior
     # POCS-TV through the host API (numpy in and out, copies included), as minTV is called
     from tigre_b200.utilities.minTV import minTV
     host = vol.cpu().numpy()
