@@ -664,7 +664,11 @@ int launch_siddon_cells(TigrePlan* P, const void* vol_z, int vdt, void* proj, in
     a.zpad = P->cells_zpad;
     const int nv = P->d.nV;
     // rows per thread: 8 (256 rows per warp, 4 resident blocks per SM) for tall detectors
-    const int R = nv >= 512 ? 8 : (nv >= 256 ? 4 : 2);
+    int R = nv >= 512 ? 8 : (nv >= 256 ? 4 : 2);
+    if (const char* e = std::getenv("TIGRE_B200_SIDDON_ROWS")) {   // tuning hook: 2, 4 or 8
+        const int r = std::atoi(e);
+        if (r == 2 || r == 4 || r == 8) R = r;
+    }
     static const int vtile_env = [] {
         const char* e = std::getenv("TIGRE_B200_SIDDON_VIEW_TILE");   // tuning hook
         return e ? std::max(1, std::atoi(e)) : 0;
