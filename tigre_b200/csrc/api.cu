@@ -47,22 +47,26 @@ void layouts_needed(const TigrePlan* p, int a0, int a1, bool& l0, bool& l1) {
     for (int i = a0; i < a1; ++i) (p->h_siddon[i].layout ? l1 : l0) = true;
 }
 
-}  // namespace
+// Working copies of the volume that the forward projectors read, built once for a range of
+// views and reused by every launch over sub-ranges of it (the host pipeline projects in view
+// chunks).  Lives in the plan's scratch until the next plan_scratch call.
+struct AxWork {
+    enum Mode { CELLS, COLUMNS, GENERAL, INTERP } mode = GENERAL;
+    const void* vx = nullptr;
+    const void* vy = nullptr;
+    const void* qx = nullptr;
+    const void* qy = nullptr;
+    int vdt = TIGRE_F32;   // element type the kernels read
+};
 
-extern "C" {
-
-int tigre_ax(TigrePlan* plan, const void* d_vol, int vdt, void* d_proj, int pdt, int projector, int a0, int a1,
-             void* stream) {
-    if (int rc = check_range(plan, a0, a1)) return rc;
-    if (!d_vol || !d_proj) return fail(TIGRE_ERR_BAD_ASSERT, "null device pointer");
-    if (!dtype_ok(vdt) || !dtype_ok(pdt)) return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype");
-    DeviceGuard g(plan->device);
-    cudaStream_t st = (cudaStream_t)stream;
+int ax_prepare(TigrePlan* plan, const void* d_vol, int vdt, int projector, int a0, int a1, cudaStream_t st,
+               AxWork* w) {
     const Dims& d = plan->d;
     bool l0, l1;
     layouts_needed(plan, a0, a1, l0, l1);
     const size_t es = dtype_size(vdt);
     int rc = TIGRE_SUCCESS;
+    w->vdt = vdt;
     if (projector == TIGRE_PROJ_SIDDON && plan->columns) {
         // z-fast working copy; the cell-interval kernel needs deeper zero pads
         const int zpad = plan->cells_zpad > 0 ? plan->cells_zpad : 1;
@@ -72,29 +76,34 @@ int tigre_ax(TigrePlan* plan, const void* d_vol, int vdt, void* d_proj, int pdt,
             float* sf = (float*)plan_scratch(plan, (size_t)d.nX * d.nY * (d.nZ + 2 * zpad) * sizeof(float), st, &rc);
             if (rc) return rc;
             if ((rc = launch_make_zfast_f32(d_vol, vdt, sf, d.nX, d.nY, d.nZ, zpad, st))) return rc;
-            return launch_siddon_cells(plan, sf, TIGRE_F32, d_proj, pdt, a0, a1, st);
+            w->mode = AxWork::CELLS;
+            w->vx = sf;
+            w->vdt = TIGRE_F32;
+            return TIGRE_SUCCESS;
         }
         void* s = plan_scratch(plan, (size_t)d.nX * d.nY * (d.nZ + 2 * zpad) * es, st, &rc);
         if (rc) return rc;
         if ((rc = launch_make_zfast(d_vol, vdt, s, d.nX, d.nY, d.nZ, zpad, st))) return rc;
-        if (plan->cells_zpad > 0) return launch_siddon_cells(plan, s, vdt, d_proj, pdt, a0, a1, st);
-        return launch_siddon_columns(plan, s, vdt, d_proj, pdt, a0, a1, st);
+        w->mode = plan->cells_zpad > 0 ? AxWork::CELLS : AxWork::COLUMNS;
+        w->vx = s;
+        return TIGRE_SUCCESS;
     }
     if (projector == TIGRE_PROJ_SIDDON) {
-        const void* vx = d_vol;
-        const void* vy = nullptr;
+        w->mode = AxWork::GENERAL;
+        w->vx = d_vol;
         if (l1) {
             void* s = plan_scratch(plan, (size_t)d.nX * d.nY * d.nZ * es, st, &rc);
             if (rc) return rc;
             if ((rc = launch_make_layout(d_vol, vdt, s, d.nX, d.nY, d.nZ, 1, 0, 0, st))) return rc;
-            vy = s;
+            w->vy = s;
         }
-        return launch_siddon(plan, vx, vy, vdt, d_proj, pdt, a0, a1, st);
+        return TIGRE_SUCCESS;
     }
     if (projector == TIGRE_PROJ_INTERPOLATED) {
         // zero-padded copies (1 before, 2 after), x- and/or y-fastest; trilinear sampling reads
         // corner quads built from them (4 values per element), point sampling the copies
         // (offsets rounded to 256 bytes: the quads are read as 8- or 16-byte vectors)
+        w->mode = AxWork::INTERP;
         const size_t padded = ((size_t)(d.nX + 3) * (d.nY + 3) * (d.nZ + 3) * es + 255) / 256 * 256;
         const bool nearest = d.accuracy > 1.0;
         if (!nearest && vdt != TIGRE_F32) {
@@ -110,7 +119,10 @@ int tigre_ax(TigrePlan* plan, const void* d_vol, int vdt, void* d_proj, int pdt,
                 if ((rc = launch_make_layout(d_vol, vdt, vx, d.nX, d.nY, d.nZ, l, 1, 2, st))) return rc;
                 if ((rc = launch_make_quads_f32(vx, vdt, l ? qy : qx, d.nX, d.nY, d.nZ, l, st))) return rc;
             }
-            return launch_interp(plan, nullptr, nullptr, qx, qy, TIGRE_F32, d_proj, pdt, a0, a1, st);
+            w->qx = qx;
+            w->qy = qy;
+            w->vdt = TIGRE_F32;
+            return TIGRE_SUCCESS;
         }
         char* s = (char*)plan_scratch(plan, padded * (nearest ? 2 : 9), st, &rc);
         if (rc) return rc;
@@ -128,9 +140,38 @@ int tigre_ax(TigrePlan* plan, const void* d_vol, int vdt, void* d_proj, int pdt,
                 if ((rc = launch_make_quads(vx, vdt, l ? qy : qx, d.nX, d.nY, d.nZ, l, st))) return rc;
             }
         }
-        return launch_interp(plan, vx, vy, qx, qy, vdt, d_proj, pdt, a0, a1, st);
+        w->vx = vx;
+        w->vy = vy;
+        w->qx = qx;
+        w->qy = qy;
+        return TIGRE_SUCCESS;
     }
     return fail(TIGRE_ERR_BAD_ASSERT, "unknown projector");
+}
+
+int ax_launch(TigrePlan* plan, const AxWork& w, void* d_proj, int pdt, int a0, int a1, cudaStream_t st) {
+    switch (w.mode) {
+        case AxWork::CELLS: return launch_siddon_cells(plan, w.vx, w.vdt, d_proj, pdt, a0, a1, st);
+        case AxWork::COLUMNS: return launch_siddon_columns(plan, w.vx, w.vdt, d_proj, pdt, a0, a1, st);
+        case AxWork::GENERAL: return launch_siddon(plan, w.vx, w.vy, w.vdt, d_proj, pdt, a0, a1, st);
+        default: return launch_interp(plan, w.vx, w.vy, w.qx, w.qy, w.vdt, d_proj, pdt, a0, a1, st);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int tigre_ax(TigrePlan* plan, const void* d_vol, int vdt, void* d_proj, int pdt, int projector, int a0, int a1,
+             void* stream) {
+    if (int rc = check_range(plan, a0, a1)) return rc;
+    if (!d_vol || !d_proj) return fail(TIGRE_ERR_BAD_ASSERT, "null device pointer");
+    if (!dtype_ok(vdt) || !dtype_ok(pdt)) return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype");
+    DeviceGuard g(plan->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    AxWork w;
+    if (int rc = ax_prepare(plan, d_vol, vdt, projector, a0, a1, st, &w)) return rc;
+    return ax_launch(plan, w, d_proj, pdt, a0, a1, st);
 }
 
 int tigre_atb(TigrePlan* plan, const void* d_proj, int pdt, void* d_vol, int vdt, int backprojector, int a0, int a1,
@@ -450,17 +491,24 @@ int host_project(const float* img, const TigreGeometry* geo, float* const* resul
     void* dvol = nullptr;
     if (int rc = S->get(0, nvox * sizeof(float), &dvol)) return rc;
     if (int rc = staged_h2d(S, dvol, img, nvox * sizeof(float), S->st)) return rc;
-    // view chunks, double-buffered: D2H of chunk k (copy stream) overlaps the kernels of chunk k+1
+    // the volume's working copies, once for all views
+    AxWork work;
+    if (int rc = ax_prepare(plan, dvol, TIGRE_F32, projector, 0, nangles, S->st, &work)) return rc;
+    // view chunks, double-buffered: D2H of chunk k (copy stream) overlaps the kernels of chunk k+1.
+    // The last chunk's copy overlaps nothing, so the views are split to end on a short chunk.
     const int chunk = (int)chunk_views(npix * sizeof(float), nangles);
+    const int tail = std::max(1, chunk / 4);
     void* buf[2];
     for (int i = 0; i < 2; ++i)
         if (int rc = S->get(1 + i, (size_t)chunk * npix * sizeof(float), &buf[i])) return rc;
     cudaEvent_t drained[2] = {S->ev[0], S->ev[1]}, computed[2] = {S->ev[2], S->ev[3]};
     int k = 0;
-    for (int a = 0; a < nangles; a += chunk, ++k) {
-        const int cnt = std::min(chunk, nangles - a), b = k % 2;
+    for (int a = 0, cnt = 0; a < nangles; a += cnt, ++k) {
+        const int rem = nangles - a;
+        cnt = rem > chunk + tail ? chunk : (rem > tail && rem > chunk / 2 ? rem - tail : std::min(rem, chunk));
+        const int b = k % 2;
         if (k >= 2) TIGRE_CUDA(cudaStreamWaitEvent(S->st, drained[b], 0));
-        if (int rc = tigre_ax(plan, dvol, TIGRE_F32, buf[b], TIGRE_F32, projector, a, a + cnt, S->st)) return rc;
+        if (int rc = ax_launch(plan, work, buf[b], TIGRE_F32, a, a + cnt, S->st)) return rc;
         TIGRE_CUDA(cudaEventRecord(computed[b], S->st));
         TIGRE_CUDA(cudaStreamWaitEvent(S->st2, computed[b], 0));
         for (int i = 0; i < cnt; ++i)
