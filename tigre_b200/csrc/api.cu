@@ -537,16 +537,21 @@ int host_backproject(const float* proj, const TigreGeometry* geo, float* result,
     void* dvol = nullptr;
     if (int rc = S->get(0, nvox * sizeof(float), &dvol)) return rc;
     // projection chunks, double-buffered: H2D of chunk k+1 (copy stream) overlaps the
-    // backprojection of chunk k, which accumulates into the volume
+    // backprojection of chunk k, which accumulates into the volume.  The first chunk's copy
+    // overlaps nothing, so views that need several chunks start with one of a quarter size
+    // (views that fit one chunk keep it: a single launch sums them in one order, as the device
+    // API does).
     const int chunk = (int)chunk_views(npix * sizeof(float), nangles);
+    const int head = nangles > chunk ? std::max(1, chunk / 4) : chunk;
     void* buf[2];
     for (int i = 0; i < 2; ++i)
         if (int rc = S->get(1 + i, (size_t)chunk * npix * sizeof(float), &buf[i])) return rc;
     cudaEvent_t copied[2] = {S->ev[0], S->ev[1]}, consumed[2] = {S->ev[2], S->ev[3]};
     const int bp = matched ? TIGRE_BACKPROJ_MATCHED : TIGRE_BACKPROJ_FDK;
     int k = 0;
-    for (int a = 0; a < nangles; a += chunk, ++k) {
-        const int cnt = std::min(chunk, nangles - a), b = k % 2;
+    for (int a = 0, cnt = 0; a < nangles; a += cnt, ++k) {
+        cnt = std::min(k == 0 ? head : chunk, nangles - a);
+        const int b = k % 2;
         if (k >= 2) TIGRE_CUDA(cudaStreamWaitEvent(S->st2, consumed[b], 0));
         if (int rc = staged_h2d(S, buf[b], proj + (size_t)a * npix, (size_t)cnt * npix * sizeof(float), S->st2, 4))
             return rc;
