@@ -184,6 +184,27 @@ def _phantom_host(seed):
     return _PH[seed]
 
 
+def conv_layers():
+    """Two calls of tigre_conv3d_fwd per U-Net layer shape (128^3 x 16 -> 16 and 64^3 x 64 -> 64,
+    random BF16 inputs, ReLU) through the C ABI: the workload of the convolution profile."""
+    import ctypes as C
+    import torch
+    from tigre_b200 import _native as N
+    L = N.lib()
+    ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    for n, cin, cout in [(128, 16, 16), (64, 64, 64)]:
+        x = torch.randn(n, n, n, cin, device="cuda").to(torch.bfloat16)
+        w = (torch.randn(cout, 27 * cin, device="cuda") / 20).to(torch.bfloat16)
+        b = torch.zeros(cout, device="cuda")
+        y = torch.empty(n, n, n, cout, device="cuda", dtype=torch.bfloat16)
+        col = torch.empty(16, dtype=torch.bfloat16, device="cuda")
+        for _ in range(2):
+            N.check(L.tigre_conv3d_fwd(ptr(x), ptr(w), ptr(b), ptr(y), None, n, n, n, cin, cout, 1, ptr(col), None),
+                    "tigre_conv3d_fwd")
+        torch.cuda.synchronize()
+    print("ok")
+
+
 def max_over_ranks(dist, values, device):
     """Element-wise maximum of per-rank device times (the slowest rank sets the job time)."""
     import torch
@@ -256,9 +277,14 @@ def main():
     ap.add_argument("--views", type=int, default=0)
     ap.add_argument("--cpu-configs", action="store_true",
                     help="only time the FP64 CPU oracle on the C1 and C2 configurations and print one JSON line")
+    ap.add_argument("--conv-layers", action="store_true",
+                    help="only run two forward calls of two U-Net convolution shapes (the conv profile workload)")
     args = ap.parse_args()
     if args.cpu_configs:
         print(json.dumps(cpu_configs()))
+        return
+    if args.conv_layers:
+        conv_layers()
         return
     set_size(args.size, args.views)
     rank = int(os.environ.get("RANK", "0"))

@@ -91,7 +91,7 @@ unsigned long long tigre_launch_count(void);
  * ------------------------------------------------------------------------- */
 
 /* Siddon ray-driven cone-beam projection.  Replaces siddon_ray_projection
- * (Common/CUDA/Siddon_projection.hpp:97, Siddon_projection.cu:271).
+ * (Common/CUDA/Siddon_projection.hpp:54, Siddon_projection.cu:271).
  * img: (nVoxelZ, nVoxelY, nVoxelX) float32; result[i]: projection i, (nDetecV, nDetecU);
  * angles: (nangles, 3) ZYZ Euler angles. */
 int tigre_siddon_ray_projection(const float* img, const TigreGeometry* geo, float* const* result,
@@ -182,8 +182,11 @@ void tigre_plan_destroy(TigrePlan* plan);
 /* Bytes of device scratch currently held by the plan. */
 long long tigre_plan_scratch_bytes(const TigrePlan* plan);
 /* Synchronises the plan's device and returns its kernel status word (0 = ok; bit 0:
- * a bounded wait inside a kernel expired, results of that call are invalid).
- * reset != 0 clears it. */
+ * a bounded wait inside a kernel expired, results of that call are invalid; bit 1: the
+ * cell-interval Siddon kernel met a ray outside the z bound computed at plan time and
+ * wrote 0 for it).  reset != 0 clears it. */
+#define TIGRE_STATUS_WAIT_EXPIRED 1
+#define TIGRE_STATUS_RAY_DROPPED 2
 int tigre_plan_status(TigrePlan* plan, int reset);
 
 /* Forward projection of d_vol (nZ,nY,nX) into d_proj ((angle_end-angle_begin), nV, nU)
@@ -201,8 +204,30 @@ int tigre_atb(TigrePlan* plan, const void* d_proj, int proj_dtype, void* d_vol, 
 int tigre_atb_ex(TigrePlan* plan, const void* d_proj, int proj_dtype, void* d_vol, int vol_dtype, int backprojector,
                  int angle_begin, int angle_end, int accumulate, void* stream);
 
-/* Frees the device buffers and plans that the host entry points keep between calls. */
+/* Frees the device buffers and plans that the host entry points keep between calls, and
+ * forgets the device addresses of this library's fixed device arrays (call it after a
+ * cudaDeviceReset before the next call into the library). */
 void tigre_release_cache(void);
+
+/* Library options (no counterpart in the reference).  They select kernel variants for
+ * diagnosis and testing, set how the host entry points move data, or make one launch fail
+ * in a controlled way for the failure-detection tests.  Options read when a plan is
+ * created (SIDDON_KERNEL, BP_BOX, BP_KERNEL) apply to plans created afterwards; the host
+ * entry points keep plans between calls, so call tigre_release_cache() after changing
+ * one.  tigre_set_option returns the previous value (or -1 with TIGRE_ERR_BAD_ASSERT in
+ * tigre_last_error for an unknown option). */
+#define TIGRE_OPT_SIDDON_KERNEL 1    /* 0 auto; 1 stepped column kernel instead of the cell-interval one; 2 the generic per-ray kernel */
+#define TIGRE_OPT_BP_BOX 2           /* 0 auto; else (BU << 16) | BV: the staged backprojector's patch box */
+#define TIGRE_OPT_BP_KERNEL 3        /* 0 auto; 1 the plain global-load backprojector instead of the TMA-staged one */
+#define TIGRE_OPT_HOST_CHUNK_VIEWS 4 /* 0 auto (~192 MB of projections); else views per host<->device chunk */
+#define TIGRE_OPT_HOST_STAGING 5     /* -1 auto; else a bit mask of the copies staged through pinned buffers:
+                                        1 volume uploads, 2 volume downloads, 4 backprojector chunk uploads,
+                                        8 backprojector volume download */
+#define TIGRE_OPT_BP_SKIP_COPY 6     /* -1 off; else the staged backprojector issues no copy for this view index
+                                        of every launch, so the wait for it runs out: the kernel then sets the
+                                        plan status and the call returns TIGRE_ERR_CUDA (failure-detection test) */
+long long tigre_set_option(int option, long long value);
+long long tigre_get_option(int option);
 
 /* Sum over all rays of the number of Siddon voxel segments (FP64 ray setup only,
  * no traversal); the algorithmic-bytes count of the Siddon roofline. */
@@ -224,7 +249,9 @@ int tigre_tv_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha
  * max_iter <= 4096 (larger values return TIGRE_ERR_BAD_ASSERT).  All calls on a device
  * share that array: calls that overlap in time on one device race and must be
  * serialised by the caller.  The first call on each device looks up the array's
- * address with that device current; make it before any stream capture. */
+ * address with that device current; make it before any stream capture.  After a
+ * cudaDeviceReset the cached address is stale: call tigre_release_cache() first, which
+ * makes the next call look it up again. */
 int tigre_tv_pocs_noalloc(void* d_img, int dtype, long nx, long ny, long nz, float alpha, int max_iter,
                           float* d_work, void* stream);
 /* Device counterparts of tigre_aw_pocs_tv and tigre_piccs_tv, in place on d_img; d_work:

@@ -2,7 +2,7 @@
 // libtigre_b200.so with the exact signatures (and therefore the same mangled
 // symbols) that TIGRE's Cython extensions bind:
 //
-//   Common/CUDA/Siddon_projection.hpp:97          siddon_ray_projection
+//   Common/CUDA/Siddon_projection.hpp:54          siddon_ray_projection
 //   Common/CUDA/ray_interpolated_projection.hpp:55 interpolation_projection
 //   Common/CUDA/voxel_backprojection.hpp:52       voxel_backprojection
 //   Common/CUDA/voxel_backprojection2.hpp:57      voxel_backprojection2
@@ -69,18 +69,19 @@ int voxel_backprojection2(float* projections, Geometry geo, float* result, float
                           const GpuIds& gpuids);
 int voxel_backprojection_parallel(float* projections, Geometry geo, float* result, float const* const alphas,
                                   int nalpha, const GpuIds& gpuids);
-// The reference returns void here; errors are reported on stderr and leave dst unchanged.
+// The reference returns void here (and exits the process on an error); these report an error
+// on stderr and fill dst (pfOut) with NaN, so that a failure cannot pass for a result.
 void pocs_tv(float* img, float* dst, float alpha, const long* image_size, int maxIter, const GpuIds& gpuids);
 // Common/CUDA/RandomNumberGenerator.hpp: Poisson (+ Gaussian) noise, seed 1234 on every call.
 void poisson_1d(const float* pfIn, size_t uiLen, float* pfOut, const GpuIds& gpuids);
 void poisson_gaussian_1d(const float* pfPoissonL, size_t uiLen, float fGaussMu, float fGaussSigma, float* pfOut,
                          GpuIds& gpuids);
-// Common/CUDA/GD_AwTV.hpp:58 and PICCS.hpp:58; void like the reference, errors on stderr.
+// Common/CUDA/GD_AwTV.hpp:58 and PICCS.hpp:58; void like the reference, errors on stderr, dst NaN.
 void aw_pocs_tv(float* img, float* dst, float alpha, const long* image_size, int maxIter, const float delta,
                 const GpuIds& gpuids);
 void piccs_tv(const float* img, const float* prior, float* dst, float alpha, float ratio, const long* image_size,
               int maxIter, const GpuIds& gpuids);
-// Common/CUDA/tv_proximal.hpp:52: TV denoising (im3ddenoise); void like the reference, errors on stderr.
+// Common/CUDA/tv_proximal.hpp:52: TV denoising (im3ddenoise); void like the reference, errors on stderr, dst NaN.
 void tvdenoising(float* src, float* dst, float lambda, const float* spacing, const long* image_size, int maxIter,
                 const GpuIds& gpuids);
 

@@ -20,7 +20,9 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
-REFERENCE_CUDA = "/root/reference/Common/CUDA"
+# the TIGRE source tree (read in place); TIGRE_REFERENCE overrides where it lives
+REFERENCE_ROOT = os.environ.get("TIGRE_REFERENCE", "/root/reference")
+REFERENCE_CUDA = os.path.join(REFERENCE_ROOT, "Common", "CUDA")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -1,6 +1,6 @@
 // extern "C" shim over the reference's own C++ entry points.
 //
-// TEST INFRASTRUCTURE ONLY.  oracle/build_ref.py compiles this file together
+// TEST INFRASTRUCTURE ONLY.  oracle/build.py (build_ref) compiles this file together
 // with the reference's CUDA sources (read in place from the TIGRE tree, never
 // copied) into oracle/_ref/libref_{ax,atb,tv}.so, grouped exactly as the
 // reference's own Python extensions group them (setup.py:347-433).  The

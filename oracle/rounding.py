@@ -42,6 +42,8 @@ def bf16_bits_stochastic(v32, r16):
     b = np.ascontiguousarray(v32, dtype=np.float32).view(np.uint32).astype(np.uint64)
     special = (b & 0x7F800000) == 0x7F800000
     out = (b + r16.astype(np.uint64)) >> 16
+    # a finite value rounded past the largest finite BF16 saturates to it, keeping its sign
+    out = np.where((out & 0x7F80) == 0x7F80, ((b >> 16) & 0x8000) | 0x7F7F, out)
     return np.where(special, bf16_bits_nearest(v32).astype(np.uint64), out).astype(np.uint16)
 
 

@@ -97,3 +97,14 @@ def test_ax_input_validation():
         tigre.Ax(np.zeros((4, 5, 7), np.float32), g, np.zeros(2))
     with pytest.raises(ValueError):
         tigre.Atb(np.zeros((3, 7, 8), np.float32), g, np.zeros(2))
+
+
+def test_options_round_trip_without_a_device(native_lib):
+    from tigre_b200 import _native as N
+    assert native_lib.tigre_get_option(N.OPT_HOST_STAGING) == -1
+    assert native_lib.tigre_get_option(N.OPT_BP_SKIP_COPY) == -1
+    with N.option(N.OPT_HOST_CHUNK_VIEWS, 7):
+        assert native_lib.tigre_get_option(N.OPT_HOST_CHUNK_VIEWS) == 7
+    assert native_lib.tigre_get_option(N.OPT_HOST_CHUNK_VIEWS) == 0
+    assert native_lib.tigre_set_option(99, 1) == -1
+    assert "unknown option" in N.last_error()

@@ -239,31 +239,34 @@ def test_empty_and_missing_rays():
 def test_staged_backprojector_fallback_and_status():
     """Blocks whose footprint does not fit the shared-memory box take the bounds-checked
     global path; both paths agree with the oracle and leave the status word clean."""
-    import os
-    import subprocess
-    import sys
-    code = r"""
-import numpy as np, torch, sys
-sys.path.insert(0, '.')
-from tests import geometries as G
-from oracle import oracle as O
-from tigre_b200 import _native as N, projectors as P
-geo, ang = G.c1_geometry(), G.angles(30)
-img = G.phantom((64, 64, 64))
-proj = O.ax(img, geo, ang, 'Siddon')
-plan = N.get_plan(N.checked_geometry(geo, ang), 0)
-for bt in ('FDK', 'matched'):
-    got = P.atb(torch.from_numpy(proj).cuda(), plan, bt).cpu().numpy()
-    ref = O.atb(proj, geo, ang, bt)
-    mx, l2 = G.rel_err(got, ref)
-    assert mx <= 1e-5 and l2 <= 1e-5, (bt, mx, l2)
-assert plan.status() == 0
-print('ok')
-"""
-    env = dict(os.environ, TIGRE_B200_BP_BOX="8x4")
-    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env,
-                       cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))), timeout=600)
-    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
+    import torch
+    from tigre_b200 import _native as N, projectors as P
+    geo, ang = G.c1_geometry(), G.angles(30)
+    img = G.phantom((64, 64, 64))
+    proj = O.ax(img, geo, ang, "Siddon")
+    with N.option(N.OPT_BP_BOX, (8 << 16) | 4):
+        plan = N.get_plan(N.checked_geometry(geo, ang), 0)
+        for bt in ("FDK", "matched"):
+            got = P.atb(torch.from_numpy(proj).cuda(), plan, bt).cpu().numpy()
+            mx, l2 = G.rel_err(got, O.atb(proj, geo, ang, bt))
+            assert mx <= TOL and l2 <= TOL, (bt, mx, l2)
+        assert plan.status() == 0
+
+
+def test_plain_backprojector_matches_oracle(case):
+    """The global-load backprojector (used for FP16 projections, and selected here for FP32
+    with TIGRE_OPT_BP_KERNEL) meets the same bar as the TMA-staged one."""
+    import torch
+    from tigre_b200 import _native as N, projectors as P
+    name, geo, ang, img = case
+    proj = O.ax(img, geo, ang, "Siddon")
+    with N.option(N.OPT_BP_KERNEL, 1):
+        plan = N.get_plan(N.checked_geometry(geo, ang), 0)
+        for bt in ("FDK", "matched"):
+            got = P.atb(torch.from_numpy(proj).cuda(), plan, bt).cpu().numpy()
+            mx, l2 = G.rel_err(got, O.atb(proj, geo, ang, bt))
+            assert mx <= TOL and l2 <= TOL, (name, bt, mx, l2)
+        assert plan.status() == 0
 
 
 def test_status_word_clean_after_projectors(case):
@@ -302,58 +305,38 @@ def test_atb_accumulate_over_view_chunks(case):
 def test_host_pipeline_with_small_chunks():
     """The host entry points stream views through two device buffers; with 4-view chunks
     (and a last partial chunk) the results equal the single-chunk call and the oracle."""
-    import os
-    import subprocess
-    import sys
-    code = r"""
-import numpy as np, sys
-sys.path.insert(0, '.')
-from tests import geometries as G
-from oracle import oracle as O
-import tigre_b200 as tigre
-geo, ang = G.odd_geometry(), G.angles(23, full=np.pi * 1.3)
-img = G.phantom(tuple(int(v) for v in geo.nVoxel), seed=5)
-for _ in range(2):
-    p = tigre.Ax(img, geo, ang, 'Siddon')
-    r = O.ax(img, geo, ang, 'Siddon')
-    mx, l2 = G.rel_err(p, r); assert mx <= 1e-5 and l2 <= 1e-5, ('ax', mx, l2)
-    for bt in ('FDK', 'matched'):
-        v = tigre.Atb(r, geo, ang, bt)
-        mx, l2 = G.rel_err(v, O.atb(r, geo, ang, bt)); assert mx <= 1e-5 and l2 <= 1e-5, (bt, mx, l2)
-print('ok')
-"""
-    env = dict(os.environ, TIGRE_B200_HOST_CHUNK_VIEWS="4")
-    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env,
-                       cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))), timeout=600)
-    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
+    import tigre_b200 as tigre
+    from tigre_b200 import _native as N
+    geo, ang = G.odd_geometry(), G.angles(23, full=np.pi * 1.3)
+    img = G.phantom(tuple(int(v) for v in geo.nVoxel), seed=5)
+    with N.option(N.OPT_HOST_CHUNK_VIEWS, 4):
+        for _ in range(2):
+            p = tigre.Ax(img, geo, ang, "Siddon")
+            r = O.ax(img, geo, ang, "Siddon")
+            mx, l2 = G.rel_err(p, r)
+            assert mx <= TOL and l2 <= TOL, ("ax", mx, l2)
+            for bt in ("FDK", "matched"):
+                v = tigre.Atb(r, geo, ang, bt)
+                mx, l2 = G.rel_err(v, O.atb(r, geo, ang, bt))
+                assert mx <= TOL and l2 <= TOL, (bt, mx, l2)
 
 
-def test_column_kernel_without_cell_intervals():
-    """TIGRE_B200_NO_CELLS=1 keeps the stepped column kernel (one-crossing variant) on the
-    axial geometries; it must meet the same bar as the default cell-interval kernel."""
-    import os
-    import subprocess
-    import sys
-    code = r"""
-import numpy as np, torch, sys
-sys.path.insert(0, '.')
-from tests import geometries as G
-from oracle import oracle as O
-from tigre_b200 import _native as N, projectors as P
-for mk, ang in ((G.c1_geometry, G.angles(40)), (G.odd_geometry, G.angles(23, full=np.pi * 1.3))):
-    geo = mk()
-    img = G.phantom(tuple(int(v) for v in geo.nVoxel), seed=4)
-    plan = N.get_plan(N.checked_geometry(geo, ang), 0)
-    got = P.ax(torch.from_numpy(img).cuda(), plan, 'Siddon').cpu().numpy()
-    mx, l2 = G.rel_err(got, O.ax(img, geo, ang, 'Siddon'))
-    assert mx <= 1e-5 and l2 <= 1e-5, (mx, l2)
-    assert plan.status() == 0
-print('ok')
-"""
-    env = dict(os.environ, TIGRE_B200_NO_CELLS="1")
-    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env,
-                       cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))), timeout=600)
-    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_other_siddon_kernels_match_oracle(kernel):
+    """TIGRE_OPT_SIDDON_KERNEL 1 keeps the stepped column kernel (one-crossing variant) and 2
+    the generic per-ray kernel on the axial geometries; both meet the bar of the default
+    cell-interval kernel."""
+    import torch
+    from tigre_b200 import _native as N, projectors as P
+    with N.option(N.OPT_SIDDON_KERNEL, kernel):
+        for mk, ang in ((G.c1_geometry, G.angles(40)), (G.odd_geometry, G.angles(23, full=np.pi * 1.3))):
+            geo = mk()
+            img = G.phantom(tuple(int(v) for v in geo.nVoxel), seed=4)
+            plan = N.get_plan(N.checked_geometry(geo, ang), 0)
+            got = P.ax(torch.from_numpy(img).cuda(), plan, "Siddon").cpu().numpy()
+            mx, l2 = G.rel_err(got, O.ax(img, geo, ang, "Siddon"))
+            assert mx <= TOL and l2 <= TOL, (kernel, mx, l2)
+            assert plan.status() == 0
 
 
 @pytest.mark.parametrize("dt", ["bfloat16", "float16"])

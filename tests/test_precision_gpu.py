@@ -45,6 +45,29 @@ def test_sart_update_bit_exact(dtype, rounding, shape, noneg):
     np.testing.assert_array_equal(xs.float().cpu().numpy(), want)
 
 
+@pytest.mark.parametrize("dtype", ["bfloat16", "float16"])
+def test_stochastic_rounding_stays_finite_near_the_largest_value(dtype):
+    """Values just below the largest finite 16-bit number, pushed up by an update, stay finite
+    under stochastic rounding (both storage types saturate like nearest rounding does not)."""
+    import torch
+    from tigre_b200 import projectors as P
+    top = float(torch.finfo(getattr(torch, dtype)).max)
+    x = np.full((2, 8, 16), top, np.float32)
+    x[1] *= -1.0
+    bp = np.zeros_like(x)
+    bp[0] = top * 2 ** -9        # below one ulp of the largest value: rounds up or stays
+    bp[1] = -top * 2 ** -9
+    v = np.ones((8, 16), np.float32)
+    xs = torch.from_numpy(x).cuda().to(getattr(torch, dtype))
+    for step in range(4):
+        P.sart_update_(xs, torch.from_numpy(bp).cuda(), torch.from_numpy(v).cuda(), 1.0, False, "stochastic",
+                       seed=3, step=step)
+    got = xs.float().cpu().numpy()
+    assert np.isfinite(got).all()
+    want = R.sart_update(x, bp, v, 1.0, False, dtype, "stochastic", seed=3, step=0)
+    assert np.isfinite(want).all()
+
+
 def test_sart_update_matches_reference_expression_fp32():
     """FP32: the fused kernel equals res + lmbda * 1.0 / V * bp followed by clip(min=0), evaluated
     as numpy evaluates it (iterative_recon_alg.py:389-401, :344-345)."""

@@ -5,6 +5,7 @@ loads it and fails loudly when it is missing -- there is no fallback path.
 """
 from __future__ import annotations
 
+import contextlib
 import copy
 import ctypes as C
 import hashlib
@@ -21,6 +22,9 @@ ROUND_NEAREST, ROUND_STOCHASTIC = 0, 1
 PROJ_SIDDON, PROJ_INTERPOLATED = 0, 1
 BACKPROJ_FDK, BACKPROJ_MATCHED = 0, 1
 PLAN_PARALLEL = 1
+STATUS_WAIT_EXPIRED, STATUS_RAY_DROPPED = 1, 2
+# library options (tigre_set_option)
+OPT_SIDDON_KERNEL, OPT_BP_BOX, OPT_BP_KERNEL, OPT_HOST_CHUNK_VIEWS, OPT_HOST_STAGING, OPT_BP_SKIP_COPY = 1, 2, 3, 4, 5, 6
 
 _FP = C.POINTER(C.c_float)
 
@@ -85,6 +89,8 @@ _SIGS = {
     "tigre_atb_ex": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                C.c_int, C.c_void_p]),
     "tigre_release_cache": (None, []),
+    "tigre_set_option": (C.c_longlong, [C.c_int, C.c_longlong]),
+    "tigre_get_option": (C.c_longlong, [C.c_int]),
     "tigre_siddon_count_segments": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "tigre_interp_count_samples": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "tigre_tv_pocs": (C.c_int, [C.c_void_p, C.c_int, C.c_long, C.c_long, C.c_long, C.c_float, C.c_int, C.c_void_p,
@@ -269,6 +275,28 @@ def get_plan(geo_checked, device=0) -> Plan:
 
 def clear_plan_cache():
     _plan_cache.clear()
+
+
+def release_all():
+    """Drops this module's plans and the host entry points' cached plans and buffers."""
+    clear_plan_cache()
+    lib().tigre_release_cache()
+
+
+@contextlib.contextmanager
+def option(key, value):
+    """Sets a library option (TIGRE_OPT_*) for the duration of a block.  Plans read some
+    options when they are created, so cached plans are dropped on entry and on exit."""
+    L = lib()
+    old = L.tigre_set_option(int(key), int(value))
+    if old == -1 and L.tigre_get_option(int(key)) != int(value):
+        raise ValueError("unknown option %d: %s" % (key, last_error()))
+    release_all()
+    try:
+        yield
+    finally:
+        L.tigre_set_option(int(key), int(old))
+        release_all()
 
 
 def host_empty(shape):

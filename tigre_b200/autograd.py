@@ -5,7 +5,10 @@ which round-trip every call through host numpy and use the FDK backprojector as
 the backward of Ax (:64).  Here everything stays on the GPU and:
 
 * AxFunction.backward = matched backprojection (A^T), the adjoint pair;
-* AtbFunction.backward = Siddon forward projection;
+* AtbFunction.backward = Siddon forward projection, the adjoint of the matched
+  backprojector.  The FDK backprojector's weights (DSO/U)^2 have no forward
+  counterpart here, so AtbFunction accepts only backprojection_type "matched";
+  FDK backprojection is a reconstruction step, not an operator to differentiate;
 * TVFunction.forward = sum_i |grad f_i| (the TV of pocs_tv's boundary rule),
   backward = grad_output * dTV/df from the hand-written gradient kernel
   (GD_TV.cu:117-143 formula).
@@ -49,6 +52,9 @@ class AxFunction(torch.autograd.Function):
 class AtbFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, proj, plan, backprojection_type="matched"):
+        if backprojection_type != "matched":
+            raise ValueError("AtbFunction differentiates the matched backprojector only (its adjoint is the "
+                             "Siddon projector); got backprojection_type=%r" % (backprojection_type,))
         ctx.plan = plan
         return _batched(lambda p: P.atb(p, plan, backprojection_type, out_dtype=torch.float32), proj.detach(),
                         plan.vol_shape)
@@ -95,6 +101,9 @@ class At(torch.nn.Module):
 
     def __init__(self, geo, angles, gpuids=None, backprojection_type="matched"):
         super().__init__()
+        if backprojection_type != "matched":
+            raise ValueError("At is the matched backprojector (the adjoint of the Siddon A); "
+                             "got backprojection_type=%r" % (backprojection_type,))
         dev = 0 if not gpuids else int(list(getattr(gpuids, "devices", gpuids))[0])
         self.plan = N.get_plan(N.checked_geometry(geo, angles), dev)
         self.backprojection_type = backprojection_type

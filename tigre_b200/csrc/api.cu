@@ -360,7 +360,7 @@ constexpr size_t kStageBytes = (size_t)64 << 20;
 constexpr size_t kStageMin = (size_t)32 << 20;
 constexpr unsigned kStageThreads = 8;
 
-// which (bit mask TIGRE_B200_STAGING, default kStageDefault): 1 uploads of a volume, 2 downloads
+// which (bit mask, option TIGRE_OPT_HOST_STAGING, default kStageDefault): 1 uploads of a volume, 2 downloads
 // of a volume, 4 the backprojector's projection-chunk uploads, 8 the backprojector's volume
 // download.  Measured at 512^3 on B200 (host call, best of three): the POCS-TV call takes
 // 175 ms direct, 146 ms with staged uploads and 62 ms with staged uploads and downloads; the
@@ -369,8 +369,8 @@ constexpr unsigned kStageThreads = 8;
 // already overlap the kernels), so the backprojector keeps the driver's path.
 constexpr int kStageDefault = 3;
 bool staging_on(int which) {
-    const char* e = getenv("TIGRE_B200_STAGING");
-    const int mask = e ? atoi(e) : kStageDefault;
+    const long long o = option(TIGRE_OPT_HOST_STAGING);
+    const long long mask = o >= 0 ? o : kStageDefault;
     return (mask & which) != 0;
 }
 
@@ -468,11 +468,22 @@ DeviceState* state(int dev) {
     return g_states[dev];
 }
 
-// Views per host<->device chunk: ~192 MB of projections, or TIGRE_B200_HOST_CHUNK_VIEWS.
+// Views per host<->device chunk: ~192 MB of projections, or option TIGRE_OPT_HOST_CHUNK_VIEWS.
 size_t chunk_views(size_t per_view_bytes, int nangles) {
     size_t c = ((size_t)192 << 20) / std::max<size_t>(per_view_bytes, 1);
-    if (const char* e = getenv("TIGRE_B200_HOST_CHUNK_VIEWS")) c = (size_t)std::max(1, atoi(e));
+    if (const long long o = option(TIGRE_OPT_HOST_CHUNK_VIEWS)) c = (size_t)std::max(1LL, o);
     return std::max<size_t>(1, std::min<size_t>((size_t)nangles, c));
+}
+
+// The plan's status word after the work queued on st, cleared for the next call; stream-ordered
+// (a copy into pageable memory returns once it is done), so no device-wide synchronisation.
+int take_status(TigrePlan* plan, cudaStream_t st, int* out) {
+    int v = 0;
+    TIGRE_CUDA(cudaMemcpyAsync(&v, plan->d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TIGRE_CUDA(cudaStreamSynchronize(st));
+    TIGRE_CUDA(cudaMemsetAsync(plan->d_status, 0, sizeof(int), st));
+    *out = v;
+    return TIGRE_SUCCESS;
 }
 
 int host_project(const float* img, const TigreGeometry* geo, float* const* result, const float* angles, int nangles,
@@ -490,6 +501,7 @@ int host_project(const float* img, const TigreGeometry* geo, float* const* resul
     const size_t nvox = (size_t)d.nX * d.nY * d.nZ, npix = (size_t)d.nU * d.nV;
     void* dvol = nullptr;
     if (int rc = S->get(0, nvox * sizeof(float), &dvol)) return rc;
+    TIGRE_CUDA(cudaMemsetAsync(plan->d_status, 0, sizeof(int), S->st));   // this call's launches alone set it
     if (int rc = staged_h2d(S, dvol, img, nvox * sizeof(float), S->st)) return rc;
     // the volume's working copies, once for all views
     AxWork work;
@@ -518,6 +530,11 @@ int host_project(const float* img, const TigreGeometry* geo, float* const* resul
     }
     TIGRE_CUDA(cudaStreamSynchronize(S->st2));
     TIGRE_CUDA(cudaStreamSynchronize(S->st));
+    // the cell-interval kernel drops (writes 0 for) a ray outside the z bound of the plan
+    int status = 0;
+    if (int rc = take_status(plan, S->st, &status)) return rc;
+    if (status & TIGRE_STATUS_RAY_DROPPED)
+        return fail(TIGRE_ERR_CUDA, "projection: a ray left the z range computed at plan time (its value is invalid)");
     return TIGRE_SUCCESS;
 }
 
@@ -548,6 +565,7 @@ int host_backproject(const float* proj, const TigreGeometry* geo, float* result,
         if (int rc = S->get(1 + i, (size_t)chunk * npix * sizeof(float), &buf[i])) return rc;
     cudaEvent_t copied[2] = {S->ev[0], S->ev[1]}, consumed[2] = {S->ev[2], S->ev[3]};
     const int bp = matched ? TIGRE_BACKPROJ_MATCHED : TIGRE_BACKPROJ_FDK;
+    TIGRE_CUDA(cudaMemsetAsync(plan->d_status, 0, sizeof(int), S->st));   // this call's launches alone set it
     int k = 0;
     for (int a = 0, cnt = 0; a < nangles; a += cnt, ++k) {
         cnt = std::min(k == 0 ? head : chunk, nangles - a);
@@ -562,7 +580,9 @@ int host_backproject(const float* proj, const TigreGeometry* geo, float* result,
     }
     if (int rc = staged_d2h(S, result, dvol, nvox * sizeof(float), S->st, 8)) return rc;
     TIGRE_CUDA(cudaStreamSynchronize(S->st2));
-    if (tigre_plan_status(plan, 1) != 0) return fail(TIGRE_ERR_CUDA, "backprojection: a bounded wait expired");
+    int status = 0;
+    if (int rc = take_status(plan, S->st, &status)) return rc;
+    if (status & TIGRE_STATUS_WAIT_EXPIRED) return fail(TIGRE_ERR_CUDA, "backprojection: a bounded wait expired");
     return TIGRE_SUCCESS;
 }
 
@@ -663,6 +683,7 @@ extern "C" void tigre_release_cache(void) {
         std::lock_guard<std::mutex> l2(g_states[i]->mu);
         g_states[i]->release();
     }
+    forget_static_addresses();
 }
 
 extern "C" {

@@ -18,8 +18,10 @@
 //    update a handful of packed FP32x2 instructions and four shared-memory
 //    loads; the matched weight along a column is a cubic fitted at four
 //    Chebyshev nodes per (column, view);
-//  * every mbarrier wait is bounded; on expiry the kernel records an error
-//    code in the plan's status word instead of hanging.
+//  * every mbarrier wait is bounded; when one expires in any thread, the whole
+//    block stops issuing copies, waits (bounded) for the copies already in
+//    flight, records TIGRE_STATUS_WAIT_EXPIRED in the plan's status word and
+//    exits without writing, instead of hanging.
 // A (block, view) whose footprint does not fit the box (possible for strongly
 // magnified geometries) falls back to bounds-checked global loads.
 
@@ -51,6 +53,7 @@ struct BPKArgs {
     float dVZ;
     float scale;
     int accumulate;       // add into the existing volume instead of overwriting it
+    int skip_view;        // failure-detection test: no copy is issued for this local view (-1: none)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -141,7 +144,10 @@ __device__ __forceinline__ void plan_patch(const BPKArgs& p, const CUtensorMap* 
         info[1] = v0;
         info[2] = fits ? 1 : 0;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (fits) {
+        if (la == p.skip_view) {
+            // failure-detection test: neither a copy nor an arrival, so the wait for this view
+            // runs out with nothing in flight
+        } else if (fits) {
             const uint32_t bytes = (uint32_t)(p.BU * p.BV * sizeof(TP));
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
             asm volatile(
@@ -216,12 +222,11 @@ __global__ void __launch_bounds__(TXY* TXY, 2) bp_tma_kernel(const __grid_consta
     for (int k = 0; k < VZ; ++k) acc[k] = 0.f;
     const TP* Pg = (const TP*)p.proj;
     const float pumax = (float)(p.BU - 2), pvmax = (float)(p.BV - 2);
-    bool failed = false;
+    int failed_at = -1;   // block-uniform: the view whose wait expired in some thread
     for (int la = 0; la < p.na; ++la) {
         const int s = la & 1;
         const uint32_t bar = s ? bar1 : bar0;
-        // after one expired wait the block stops waiting (its result is flagged invalid)
-        if (!failed && !mbar_wait(bar, (uint32_t)((la >> 1) & 1))) failed = true;
+        const bool ok = mbar_wait(bar, (uint32_t)((la >> 1) & 1));
         const TP* patch = s ? buf1 : buf0;
         const uint32_t patch_u32 = s ? buf1_u32 : buf0_u32;
         const int u0 = info[s][0], v0 = info[s][1], fits = info[s][2];
@@ -376,14 +381,25 @@ __global__ void __launch_bounds__(TXY* TXY, 2) bp_tma_kernel(const __grid_consta
                 }
             }
         }
-        __syncthreads();   // everyone is done with buffer s
+        // everyone is done with buffer s; a wait that expired in any thread stops the whole
+        // block before buffer s is refilled or its barrier re-armed
+        if (__syncthreads_or(!ok)) {
+            failed_at = la;
+            break;
+        }
         if (tid < 32 && la + 2 < p.na) plan_patch<TP>(p, &tmap, la + 2, x0, y0, z0, s ? buf1 : buf0, bar, info[s]);
     }
-    if (failed) {
-        // a copy may still be in flight: wait for the last phase of both buffers (bounded) before exiting
-        if (p.na > 0) mbar_wait(bar0, (uint32_t)(((p.na - 1 - ((p.na - 1) & 1)) >> 1) & 1));
-        if (p.na > 1) mbar_wait(bar1, (uint32_t)(((p.na - 1 - ((p.na - 1 + 1) & 1)) >> 1) & 1));
-        if (p.status) atomicOr(p.status, 1);
+    if (failed_at >= 0) {
+        // the copies of views failed_at and failed_at + 1 were issued and may still be in flight
+        // (failed_at + 2 was not): wait for them, bounded, so that no copy lands in the shared
+        // memory of an exited block; the block's results are not written
+        if (tid == 0) {
+            const int la = failed_at;
+            mbar_wait((la & 1) ? bar1 : bar0, (uint32_t)((la >> 1) & 1));
+            if (la + 1 < p.na) mbar_wait(((la + 1) & 1) ? bar1 : bar0, (uint32_t)(((la + 1) >> 1) & 1));
+            if (p.status) atomicOr(p.status, TIGRE_STATUS_WAIT_EXPIRED);
+        }
+        return;
     }
     if (!active) return;
     TV* V = (TV*)p.vol;
@@ -462,6 +478,8 @@ int launch_backproject_tma(TigrePlan* P, const void* proj, int pitch, int pdt, v
     a.dVZ = (float)P->d.dVZ;
     a.scale = matched ? (float)(P->d.dVX * P->d.dVY * P->d.dVZ / (P->d.dDU * P->d.dDV)) : 1.f;
     a.accumulate = accumulate;
+    const long long skip = option(TIGRE_OPT_BP_SKIP_COPY);
+    a.skip_view = (skip >= 0 && skip < na) ? (int)skip : -1;
     const bool ax = P->axial;
     if (pdt == TIGRE_F32 && vdt == TIGRE_F32) return launch_typed<float, float>(tm, a, matched, ax, st);
     if (pdt == TIGRE_BF16 && vdt == TIGRE_BF16) return launch_typed<__nv_bfloat16, __nv_bfloat16>(tm, a, matched, ax, st);

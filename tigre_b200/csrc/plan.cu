@@ -34,6 +34,17 @@ std::atomic<unsigned long long> g_launches{0};
 
 void note_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+// ---- library options (tigre_set_option) ----
+namespace {
+constexpr int kNumOptions = 7;
+// defaults: SIDDON_KERNEL 0, BP_BOX 0, BP_KERNEL 0, HOST_CHUNK_VIEWS 0, HOST_STAGING -1, BP_SKIP_COPY -1
+std::atomic<long long> g_options[kNumOptions] = {{0}, {0}, {0}, {0}, {0}, {-1}, {-1}};
+}  // namespace
+
+long long option(int key) {
+    return (key > 0 && key < kNumOptions) ? g_options[key].load(std::memory_order_relaxed) : 0;
+}
+
 int fail(int code, const std::string& msg) {
     set_error(msg);
     return code;
@@ -144,7 +155,7 @@ void cells_bounds(TigrePlan* plan) {
     // one z crossing per xy cell at most (z change per cell < 1, with margin), and pads that
     // stay a modest multiple of the volume
     const double pad = std::ceil(span) + 3.0;
-    const bool ok = slope < 0.9 && pad <= 2.0 * d.nZ + 256.0 && std::getenv("TIGRE_B200_NO_CELLS") == nullptr;
+    const bool ok = slope < 0.9 && pad <= 2.0 * d.nZ + 256.0 && option(TIGRE_OPT_SIDDON_KERNEL) == 0;
     plan->cells_zpad = ok ? (int)pad : 0;
 }
 
@@ -446,7 +457,7 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
         }
     }
     plan->axial = axial;
-    plan->columns = columns && std::getenv("TIGRE_B200_GENERIC_SIDDON") == nullptr;
+    plan->columns = columns && option(TIGRE_OPT_SIDDON_KERNEL) != 2;
     if (plan->columns) cells_bounds(plan);
 
     // ---- staged backprojector constants and patch box ----
@@ -514,18 +525,12 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
         int BV = (int)std::ceil(ext_v) + 6;
         if (BV < 4) BV = 4;
         // float rows: the pitch (mod 32 words) with the fewest estimated shared-memory wavefronts
-        // among those whose double buffer fits the 96 KB budget (tuning hook: force one residue)
+        // among those whose double buffer fits the 96 KB budget
         const int base = (std::max(need, 4) + 3) / 4 * 4;
         int BU = base;
         while (BU % 8 != 4) BU += 4;
-        int forced = -1;
-        if (const char* pm = std::getenv("TIGRE_B200_BP_PITCH_MOD32")) {
-            const int v = std::atoi(pm);
-            if (v >= 0 && v < 32 && v % 4 == 0) forced = v;
-        }
         double best = -1.0;
         for (int r = 0; r < 32; r += 4) {
-            if (forced >= 0 && r != forced) continue;
             int bu = base;
             while (bu % 32 != r) bu += 4;
             if (bu > 256 || 2.0 * bu * BV * 4 > 96.0 * 1024) continue;
@@ -544,16 +549,16 @@ int compute_frames(const TigreGeometry* g, const float* angles, int nangles, Tig
             const double c = bp_bank_cost(plan, bu, 2, bx, bz);
             if (best < 0.0 || c < best || (c == best && bu < BU16)) { best = c; BU16 = bu; }
         }
-        if (const char* ov = std::getenv("TIGRE_B200_BP_BOX")) {   // test hook: force a box (e.g. "8x4")
-            int bu = 0, bv = 0;
-            if (std::sscanf(ov, "%dx%d", &bu, &bv) == 2 && bu > 0 && bv > 0) {
+        if (const long long box = option(TIGRE_OPT_BP_BOX)) {   // forced box (tests of the fallback path)
+            const int bu = (int)((box >> 16) & 0xffff), bv = (int)(box & 0xffff);
+            if (bu > 0 && bv > 0) {
                 BU = (bu + 3) / 4 * 4;
                 BU16 = (bu + 7) / 8 * 8;
                 BV = bv;
             }
         }
         const bool ok = std::isfinite(ext_u) && std::isfinite(ext_v) && BU <= 256 && BU16 <= 256 && BV <= 256 &&
-                        2.0 * BU * BV * 4 <= 96.0 * 1024 && std::getenv("TIGRE_B200_NO_TMA") == nullptr;
+                        2.0 * BU * BV * 4 <= 96.0 * 1024 && option(TIGRE_OPT_BP_KERNEL) == 0;
         plan->bp_box_u = ok ? BU : 0;
         plan->bp_box_u16 = ok ? BU16 : 0;
         plan->bp_box_v = ok ? BV : 0;
@@ -586,7 +591,23 @@ extern "C" {
 
 const char* tigre_last_error(void) { return g_last_error.c_str(); }
 
-int tigre_version(void) { return 100; }
+int tigre_version(void) { return 101; }
+
+long long tigre_set_option(int key, long long value) {
+    if (key <= 0 || key >= kNumOptions) {
+        fail(TIGRE_ERR_BAD_ASSERT, "unknown option " + std::to_string(key));
+        return -1;
+    }
+    return g_options[key].exchange(value, std::memory_order_relaxed);
+}
+
+long long tigre_get_option(int key) {
+    if (key <= 0 || key >= kNumOptions) {
+        fail(TIGRE_ERR_BAD_ASSERT, "unknown option " + std::to_string(key));
+        return -1;
+    }
+    return g_options[key].load(std::memory_order_relaxed);
+}
 unsigned long long tigre_launch_count(void) { return tigre::g_launches.load(std::memory_order_relaxed); }
 
 int tigre_plan_create(const TigreGeometry* geo, const float* angles, int nangles, int device, TigrePlan** out) {

@@ -59,7 +59,10 @@ template <> struct Rounder<__nv_bfloat16, true> {
     static __device__ __forceinline__ __nv_bfloat16 apply(float v, uint32_t r16) {
         const uint32_t b = __float_as_uint(v);
         if ((b & 0x7F800000u) == 0x7F800000u) return __float2bfloat16_rn(v);   // Inf, NaN
-        return __ushort_as_bfloat16((unsigned short)((b + r16) >> 16));
+        const uint32_t r = (b + r16) >> 16;
+        // a finite value rounded up past the largest finite BF16 stays at it (as the FP16 path)
+        if ((r & 0x7F80u) == 0x7F80u) return __ushort_as_bfloat16((unsigned short)(((b >> 16) & 0x8000u) | 0x7F7Fu));
+        return __ushort_as_bfloat16((unsigned short)r);
     }
 };
 

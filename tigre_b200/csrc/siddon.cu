@@ -664,16 +664,8 @@ int launch_siddon_cells(TigrePlan* P, const void* vol_z, int vdt, void* proj, in
     a.zpad = P->cells_zpad;
     const int nv = P->d.nV;
     // rows per thread: 8 (256 rows per warp, 4 resident blocks per SM) for tall detectors
-    int R = nv >= 512 ? 8 : (nv >= 256 ? 4 : 2);
-    if (const char* e = std::getenv("TIGRE_B200_SIDDON_ROWS")) {   // tuning hook: 2, 4 or 8
-        const int r = std::atoi(e);
-        if (r == 2 || r == 4 || r == 8) R = r;
-    }
-    static const int vtile_env = [] {
-        const char* e = std::getenv("TIGRE_B200_SIDDON_VIEW_TILE");   // tuning hook
-        return e ? std::max(1, std::atoi(e)) : 0;
-    }();
-    const int vtile = vtile_env ? vtile_env : 64;   // flat between 32 and 128 views at 512^3 / 1024x768
+    const int R = nv >= 512 ? 8 : (nv >= 256 ? 4 : 2);
+    const int vtile = 64;   // flat between 32 and 128 views at 512^3 / 1024x768
     const int na = a1 - a0;
     const int nug = (P->d.nU + kCellWarps - 1) / kCellWarps, nbands = (nv + 32 * R - 1) / (32 * R);
     const long max_views = std::max(1L, (long)INT32_MAX / ((long)nug * nbands));

@@ -19,6 +19,10 @@ int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
 // process-wide count of kernels launched by this library (tigre_launch_count)
 void note_launches(unsigned long long n);
+// current value of a library option (TIGRE_OPT_*, tigre_set_option)
+long long option(int key);
+// forgets the cached device addresses of the library's fixed device arrays (tigre_release_cache)
+void forget_static_addresses();
 
 // after a kernel launch: check the launch and count it
 #define TIGRE_LAUNCHED()                   \

@@ -116,13 +116,9 @@ TvTiles tv_tiles(const TVDims& d, int rows) {
 
 int tv_tiled_grid(const TvTiles& t) { return std::min(t.ntiles, 148 * 8); }
 
-// rows of the tile each thread owns (1: 32 x 8 tiles, 2: 32 x 16); TIGRE_B200_TV_ROWS overrides.
-// PICCS, with two staged fields, always uses one row.
-int tv_rows(int kind) {
-    if (kind == kTvPiccs) return 1;
-    const char* e = std::getenv("TIGRE_B200_TV_ROWS");
-    return (e && std::atoi(e) == 1) ? 1 : 2;
-}
+// rows of the tile each thread owns (1: 32 x 8 tiles, 2: 32 x 16).  PICCS, with two staged
+// fields, uses one row.
+int tv_rows(int kind) { return kind == kTvPiccs ? 1 : 2; }
 
 // 1 / (sqrt(s) + eps) for s >= 0
 __device__ __forceinline__ float tv_rnorm(float s, float eps) {
@@ -470,7 +466,9 @@ int tigre_tv_piccs(void* d_img, const void* d_prior, int dtype, long nx, long ny
 // stream before use.  Calls that overlap in time on one device (other streams, other
 // host threads) therefore race on the sums and must be serialised by the caller.
 // The first call on each device looks up the array's address with that device
-// current and caches it; make that first call before any stream capture.
+// current and caches it; make that first call before any stream capture.  A device
+// reset invalidates the cached address: tigre_release_cache() forgets it, and the
+// next call looks it up again.
 constexpr int kTvPocsStaticMaxIter = 4096;   // 32 KiB
 static __device__ __align__(256) double g_tv_pocs_sums[kTvPocsStaticMaxIter];
 
@@ -495,6 +493,13 @@ int tv_pocs_static_sums(double** out) {
     return TIGRE_SUCCESS;
 }
 }  // namespace
+
+namespace tigre {
+void forget_static_addresses() {
+    std::lock_guard<std::mutex> lk(g_tv_pocs_sums_mu);
+    for (auto& a : g_tv_pocs_sums_addr) a = nullptr;
+}
+}  // namespace tigre
 
 extern "C" int tigre_tv_pocs_noalloc(void* d_img, int dtype, long nx, long ny, long nz, float alpha, int max_iter,
                                      float* d_work, void* stream) {
