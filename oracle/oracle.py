@@ -200,11 +200,14 @@ def piccs_tv(img, prior, alpha, ratio, maxiter, nthreads=0):
 
 
 # ---------------------------------------------------------------- FDK pieces --
-def fdk_filter(proj, geo, angles, filter=None, cosine=True):  # noqa: A002
+def fdk_filter(proj, geo, angles, filter=None, cosine=True, filter_scale=None,  # noqa: A002
+               stop_before_filter=False):
     """Cosine weighting + ramp filtering exactly as the reference's host path:
     single_pass_algorithms.py:186-197 then filtering.py:15-53 (scipy.fft on
     complex64, two projections per transform).  cosine=False: the ramp filter
-    alone, as fbp uses it (single_pass_algorithms.py:221)."""
+    alone, as fbp uses it (single_pass_algorithms.py:221).  filter_scale replaces
+    the angular factor 2 pi / nangles; stop_before_filter returns the cosine-weighted
+    projections."""
     from scipy.fft import fft, ifft
     g = copy.deepcopy(geo)
     g.check_geo(angles)
@@ -216,6 +219,8 @@ def fdk_filter(proj, geo, angles, filter=None, cosine=True):  # noqa: A002
     dsd, dso = float(g.DSD[0]), float(g.DSO[0])
     w = dsd / np.sqrt(dsd ** 2 + xx ** 2 + yy ** 2) if cosine else np.ones_like(xx)
     p = np.multiply(np.asarray(proj, dtype=np.float32), w).astype(np.float32)
+    if stop_before_filter:
+        return p
 
     def nextpow2(n):
         i = 1
@@ -245,7 +250,7 @@ def fdk_filter(proj, geo, angles, filter=None, cosine=True):  # noqa: A002
     filt = np.kron(np.ones((nv, 1), dtype=np.float32), filt)
     pad = int((L - nu) // 2)
     n = p.shape[0]
-    scale = (dsd / dso) * (2 * np.pi / n) / (4 * du)
+    scale = (dsd / dso) * ((2 * np.pi / n) if filter_scale is None else filter_scale) / (4 * du)
     f = np.empty((nv, L), dtype=np.complex64)
     for i in range(0, n - 1, 2):
         f.fill(0)
@@ -262,8 +267,58 @@ def fdk_filter(proj, geo, angles, filter=None, cosine=True):  # noqa: A002
     return p
 
 
-def fdk(proj, geo, angles, filter=None):  # noqa: A002
-    return atb(fdk_filter(proj, geo, angles, filter), geo, angles, "FDK")
+def parker_weights(geo, angles, q=1.0):
+    """FP64 Parker short-scan weights, (nangles, nU): Wesarg, Ebert and Bortfeld, "Parker
+    weights revisited", Med. Phys. 29(3) 2002, as TIGRE restates them in
+    MATLAB/Utilities/ParkerWeight.m:17-43 -- fan angle of each detector column along u,
+    negated when the angles increase, half fan angle delta from the outermost column
+    centres, overscan epsilon = max(span - (pi + 2 delta), 0), and the smooth step S of
+    the four transition terms.  Python/tigre/utilities/parkerweight.py:23-78 evaluates
+    the same expression (it always negates, and takes the extent of the first detector
+    axis, so it agrees for square detectors with increasing angles: pinned against it by
+    tests/golden/ref_parker.npz).  Divisions by a zero transition width follow IEEE
+    arithmetic and S maps NaN to 0, as the reference's boolean masks do."""
+    g = copy.deepcopy(geo)
+    g.check_geo(angles)
+    a = np.asarray(g.angles, dtype=np.float64)[:, 0]
+    nu, du, su = int(g.nDetector[1]), float(g.dDetector[1]), float(g.sDetector[1])
+    gam = np.arctan((np.arange(nu, dtype=np.float64) * du - su / 2 + du / 2) / float(np.mean(g.DSD)))
+    if np.all(np.diff(a) >= 0):
+        gam = -gam
+    delta = abs(gam[-1] - gam[0]) / 2
+    eps = max(abs(a[-1] - a[0]) - (np.pi + 2 * delta), 0.0)
+    beta = np.abs(a - a[0])[:, None]
+
+    def smooth_step(t):
+        inner = 0.5 * (1.0 + np.sin(np.pi * np.clip(t, -0.5, 0.5)))
+        return np.where(t >= 0.5, 1.0, np.where(np.abs(t) < 0.5, inner, 0.0))
+
+    with np.errstate(divide="ignore", invalid="ignore"):
+        wa = q * (2 * delta - 2 * gam + eps)
+        wb = q * (2 * delta + 2 * gam + eps)
+        w = 0.5 * (smooth_step(beta / wa - 0.5) + smooth_step((beta - 2 * delta + 2 * gam - eps) / wa + 0.5)
+                   - smooth_step((beta - np.pi + 2 * gam) / wb - 0.5)
+                   - smooth_step((beta - np.pi - 2 * delta - eps) / wb + 0.5))
+    return w
+
+
+def fdk(proj, geo, angles, filter=None, parker=False, z_range=None):  # noqa: A002
+    """FDK: cosine weights, optional Parker weights (parker = q, True meaning 1), ramp
+    filter, FDK-weighted backprojection.  With Parker weights the angular factor of the
+    filter scale is 2 * mean view step instead of 2 pi / nangles
+    (MATLAB/Utilities/filtering.m:23-26,47-48, the wiring of MATLAB/Algorithms/FDK.m:153-161)."""
+    if not parker:
+        return atb(fdk_filter(proj, geo, angles, filter), geo, angles, "FDK", z_range=z_range)
+    q = 1.0 if parker is True else float(parker)
+    a = np.asarray(angles, dtype=np.float64)
+    a = a[:, 0] if a.ndim == 2 else a
+    # fdk_filter applies cosine weights, then filters; Parker weights go between the two
+    W = parker_weights(geo, angles, q)
+    cos_only = fdk_filter(proj, geo, angles, filter, cosine=True, filter_scale=None, stop_before_filter=True)
+    weighted = (cos_only.astype(np.float64) * W[:, None, :]).astype(np.float32)
+    filt = fdk_filter(weighted, geo, angles, filter, cosine=False,
+                      filter_scale=2 * float(np.mean(np.abs(np.diff(a)))))
+    return atb(filt, geo, angles, "FDK", z_range=z_range)
 
 
 def fbp(proj, geo, angles, filter=None):  # noqa: A002

@@ -40,14 +40,17 @@ def main():
             print(name, "updated", sorted(keys))
             continue
         res = {}
+        want = set(GC.keys(name))
         res["siddon"], _ = ref.ax(img, geo, ang, "Siddon")
         res["interpolated"], _ = ref.ax(img, geo, ang, "interpolated")
         res["fdk"], _ = ref.atb(res["siddon"], geo, ang, "FDK")
         res["matched"], _ = ref.atb(res["siddon"], geo, ang, "matched")
-        res["pocs_tv"], _ = ref.pocs_tv(img, GC.TV_ALPHA, GC.TV_ITERS)
-        scaled = (img - img.min()) / (img - img.min()).max()
-        res["tvdenoise"], _ = ref.tvdenoise(scaled.astype(np.float32), GC.DENOISE_LAMBDA, GC.DENOISE_ITERS)
-        _tv_family(res, img, {"awtv", "piccs"})
+        if "pocs_tv" in want:
+            res["pocs_tv"], _ = ref.pocs_tv(img, GC.TV_ALPHA, GC.TV_ITERS)
+        if "tvdenoise" in want:
+            scaled = (img - img.min()) / (img - img.min()).max()
+            res["tvdenoise"], _ = ref.tvdenoise(scaled.astype(np.float32), GC.DENOISE_LAMBDA, GC.DENOISE_ITERS)
+        _tv_family(res, img, want & {"awtv", "piccs"})
         np.savez_compressed(path, **res)
         print(name, {k: v.shape for k, v in res.items()})
 

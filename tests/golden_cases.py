@@ -17,7 +17,15 @@ def piccs_prior(img):
     return (0.9 * np.roll(np.roll(img, 1, axis=2), 1, axis=1)).astype(np.float32)
 
 
-CASES = ("small", "offsets", "parallel")
+CASES = ("small", "offsets", "parallel", "rotated", "c1")
+
+# outputs stored per case (default: every output); the C1-size case keeps the projector pair only
+KEYS = {"c1": ("siddon", "interpolated", "fdk", "matched")}
+ALL_KEYS = ("siddon", "interpolated", "fdk", "matched", "pocs_tv", "tvdenoise", "awtv", "piccs")
+
+
+def keys(name):
+    return KEYS.get(name, ALL_KEYS)
 
 
 def make(name):
@@ -42,6 +50,26 @@ def make(name):
         geo.COR = 0.3
         ang = np.linspace(0.05, np.pi, 9, endpoint=False).astype(np.float32)
         img = random_ellipsoids((20, 26, 30), seed=23)
+    elif name == "rotated":
+        # detector roll/pitch/yaw, non-axial Euler angles (theta, psi), centre-of-rotation shift
+        # and origin/detector offsets: every term of the reference's geometry frames
+        geo = cone_geometry((26, 30, 34), (26 * 1.1, 30.0, 34 * 0.9), (44, 56), (0.9, 0.8))
+        geo.rotDetector = np.array((0.04, -0.03, 0.05))
+        geo.COR = 0.6
+        geo.offOrigin = np.array((0.8, 1.2, -1.0))
+        geo.offDetector = np.array((-1.1, 0.9))
+        rng = np.random.default_rng(24)
+        ang = np.zeros((11, 3), dtype=np.float32)
+        ang[:, 0] = np.linspace(0.2, 2 * np.pi, 11, endpoint=False)
+        ang[:, 1] = rng.uniform(-0.25, 0.25, 11)
+        ang[:, 2] = rng.uniform(-0.25, 0.25, 11)
+        img = random_ellipsoids((26, 30, 34), seed=24)
+    elif name == "c1":
+        # the small plain-method configuration (64^3 @ 1 mm, 128 x 128 @ 0.8 mm, DSO 1000 /
+        # DSD 1536), on 12 of its 100 views to keep the fixture small
+        geo = cone_geometry((64, 64, 64), (64.0, 64.0, 64.0), (128, 128), (0.8, 0.8))
+        ang = np.linspace(0, 2 * np.pi, 100, endpoint=False).astype(np.float32)[::9][:12]
+        img = random_ellipsoids((64, 64, 64), seed=0)
     else:
         raise KeyError(name)
     return geo, ang, img.astype(np.float32)
