@@ -137,17 +137,19 @@ def test_c4_batched_autograd_adjoint():
 
 
 def test_c4_batched_loss_central_differences():
-    """loss = |Ax - b|^2 + 1e-3 TV(x) over the batch, central differences at h = 1e-3.  The TV
-    term's backward is exact (random directions); the data term's is the matched
-    backprojector, the approximate adjoint of Siddon, so it is checked along smooth directions
-    (Gaussian blobs in every batch element) within that gap (< 6 %)."""
+    """loss = |Ax - b|^2 + 1e-3 TV(x) over the batch, central differences at h = 1e-3 along
+    smooth directions (a Gaussian blob in every batch element).  The backward of Ax is the
+    matched backprojector, the reference's adjoint of Siddon up to its weights' small mismatch,
+    so the bar is 1e-3 relative: the residual Ax0 - b is kept systematic (x0 = 1.05 x + noise)
+    so that <r, A d> is not a near-cancelling sum of signed noise, which would magnify that
+    mismatch.  The TV term's backward is exact: checked along random directions at 2e-3."""
     import torch
     from tigre_b200 import autograd as AG, projectors as P
     geo, ang, x = _c4()
     A = AG.A(geo, ang)
     g = torch.Generator("cuda").manual_seed(2)
-    b = (A(x) + 0.01 * torch.randn((8, 180, 256, 256), device="cuda", generator=g)).double()
-    x0 = x + 0.02 * torch.randn(x.shape, device="cuda", generator=g)
+    b = A(x).double()
+    x0 = 1.05 * x + 0.02 * torch.randn(x.shape, device="cuda", generator=g)
     h = 1e-3
 
     def data(v):
@@ -177,7 +179,7 @@ def test_c4_batched_loss_central_differences():
         e_data = abs(fd(data, d) - float((g_data * d).sum())) / abs(fd(data, d))
         e_all = abs(fd(loss, d) - float((g_all * d).sum())) / abs(fd(loss, d))
         print("C4 central differences: data %.3e, data + TV %.3e" % (e_data, e_all))
-        assert e_data < 0.06 and e_all < 0.06, (e_data, e_all)
+        assert e_data < 1e-3 and e_all < 1e-3, (e_data, e_all)
     # TV alone along random directions (FP64 sums; shifted away from the kink at 0 as in the
     # small-size check)
     x1 = x0 + 4.0

@@ -50,6 +50,21 @@ def _oracle_output(key, img, geo, ang, ref):
     raise KeyError(key)
 
 
+# Rays on which the reference's own Siddon output is wrong: (case, view, detector column).  On
+# the C1-size case every row of column 69 of view 2 (64.8 degrees) misses or gains part of its
+# line integral (up to 5.9 % of the maximum; 95 of 196,608 rays); an independent fine-sampled
+# line integral agrees with the oracle there (test below), so these rays are excluded from the
+# comparison -- and the exclusion must stay exactly this set.
+REFERENCE_SIDDON_DEFECTS = {"c1": [(2, 69)]}
+
+
+def _defect_mask(name, shape):
+    mask = np.zeros(shape, dtype=bool)
+    for view, col in REFERENCE_SIDDON_DEFECTS.get(name, []):
+        mask[view, :, col] = True
+    return mask
+
+
 @pytest.mark.parametrize("name", GC.CASES)
 def test_oracle_matches_reference_cuda(name):
     path = os.path.join(HERE, "golden", "ref_%s.npz" % name)
@@ -59,8 +74,56 @@ def test_oracle_matches_reference_cuda(name):
     geo, ang, img = GC.make(name)
     for k in GC.keys(name):
         tmax, tl2 = TOLS[k]
-        mx, l2 = rel_err(_oracle_output(k, img, geo, ang, ref), ref[k])
+        got = _oracle_output(k, img, geo, ang, ref)
+        want = ref[k]
+        if k == "siddon":
+            bad = _defect_mask(name, want.shape)
+            off = np.abs(got - want) > tmax * np.abs(want).max()
+            assert not (off & ~bad).any(), (name, np.argwhere(off & ~bad)[:5])
+            got, want = got[~bad], want[~bad]
+        mx, l2 = rel_err(got, want)
         assert mx <= tmax and l2 <= tl2, (name, k, mx, l2)
+
+
+def _fine_line_integral(img, alpha, v, u, geo, n=400000):
+    """Line integral of the voxelised image along one cone-beam ray by midpoint sampling (no
+    Siddon traversal): axial geometry without offsets, source at (DSO, 0, 0) rotated by alpha
+    about z, detector pixel (u, v) at x = -(DSD - DSO), u along +y, v along +z, both from the
+    detector's lower corner, volume centred at the origin."""
+    nz, ny, nx = img.shape
+    dv, du = float(geo.dDetector[0]), float(geo.dDetector[1])
+    nv, nu = int(geo.nDetector[0]), int(geo.nDetector[1])
+    vox = np.asarray(geo.dVoxel, dtype=np.float64)[::-1]          # (x, y, z) mm
+    s = np.array([geo.DSO, 0.0, 0.0])
+    p = np.array([-(geo.DSD - geo.DSO), -nu * du / 2 + du / 2 + u * du, -nv * dv / 2 + dv / 2 + v * dv])
+    c, sn = np.cos(alpha), np.sin(alpha)
+    rot = np.array([[c, -sn, 0.0], [sn, c, 0.0], [0.0, 0.0, 1.0]])
+    s, p = rot @ s, rot @ p
+    t = (np.arange(n) + 0.5) / n
+    pts = (s[None] + t[:, None] * (p - s)[None]) / vox + np.array([nx, ny, nz]) / 2.0
+    idx = np.floor(pts).astype(np.int64)
+    ok = np.all((idx >= 0) & (idx < np.array([nx, ny, nz])), axis=1)
+    vals = np.zeros(n)
+    vals[ok] = img[idx[ok, 2], idx[ok, 1], idx[ok, 0]]
+    return float(vals.sum() * np.linalg.norm(p - s) / n)
+
+
+def test_oracle_siddon_matches_fine_sampling_where_the_reference_errs():
+    """On the rays where the reference's Siddon disagrees with the oracle, a midpoint-sampled
+    line integral (4e5 samples per ray, independent of both traversals) sides with the oracle;
+    on ordinary rays of the same view all three agree."""
+    geo, ang, img = GC.make("c1")
+    ref = np.load(os.path.join(HERE, "golden", "ref_c1.npz"))["siddon"]
+    orc = O.ax(img, geo, ang, "Siddon")
+    top = float(np.abs(orc).max())
+    for view, col in REFERENCE_SIDDON_DEFECTS["c1"]:
+        for v in (2, 16, 70, 101):
+            fine = _fine_line_integral(img, float(ang[view]), v, col, geo)
+            assert abs(fine - orc[view, v, col]) <= 2e-4 * top, (v, fine, orc[view, v, col])
+            assert abs(fine - ref[view, v, col]) > 5e-3 * top, (v, fine, ref[view, v, col])
+        for v, u in ((40, 30), (90, 100)):
+            fine = _fine_line_integral(img, float(ang[view]), v, u, geo)
+            assert abs(fine - orc[view, v, u]) <= 2e-4 * top and abs(fine - ref[view, v, u]) <= 5e-4 * top
 
 
 def test_awtv_oracle_reduces_to_pocs_tv():
