@@ -218,19 +218,148 @@ def job_throughput(world, units_per_rank, seconds):
     return world * units_per_rank / seconds / 1e9
 
 
+# ------------------------------------------------------------------ CGLS time to residual --
+# The learned-vs-plain half of the metric on the warm-start configuration: 256^3 @ 1 mm random
+# ellipsoids (seed 0), 512 x 512 detector @ 0.8 mm, 90 views over 2 pi, DSO 1000 / DSD 1536.
+C5_VOX, C5_DET, C5_DDET, C5_VIEWS = 256, 512, 0.8, 90
+C5_I0 = 5e4
+C5_TOL = 1e-3
+C5_MAX_ITERS = 300
+C5_WORKLOAD = ("CGLS on 256^3 @ 1 mm, 512x512 det @ 0.8 mm, 90 views / 2pi, DSO 1000, DSD 1536; "
+               "noiseless: Siddon projections of the phantom; noisy: Poisson I0 = 5e4 (+ N(0, 0.5) counts)")
+
+
+def c5_geometry():
+    from tigre_b200.utilities.geometry import cone_geometry
+    return cone_geometry((C5_VOX,) * 3, (float(C5_VOX),) * 3, (C5_DET, C5_DET), (C5_DDET, C5_DDET),
+                         DSO=1000.0, DSD=1536.0)
+
+
+def c5_angles():
+    return np.linspace(0, 2 * np.pi, C5_VIEWS, endpoint=False).astype(np.float32)
+
+
+def c5_noise(proj_np):
+    """Noisy line integrals with the noise model of CTnoise.add (Python/tigre/utilities/
+    CTnoise.py:4-33): counts I0 exp(-p / max p), Poisson plus N(0, 0.5), back to -log(counts /
+    I0) max p; drawn with numpy's seeded generator so that both arms of the benchmark get the
+    same numbers."""
+    p = np.asarray(proj_np, dtype=np.float32)
+    pmax = float(p.max())
+    rng = np.random.default_rng(1234)
+    counts = rng.poisson(C5_I0 * np.exp(-p.astype(np.float64) / pmax)) + rng.normal(0.0, 0.5, p.shape)
+    return (-np.log(counts / C5_I0) * pmax).astype(np.float32)
+
+
+def measure_cgls():
+    """Wall time (host clock, synchronised; the whole driver: its per-iteration residual reads
+    included) of CGLS until ||b - A x|| / ||b|| meets the criterion, from a zero start and from
+    the FDK reconstruction (FDK time included).  Noiseless data: criterion 1e-3.  Noisy data:
+    the relative residual stalls at the noise level, so the criterion is the residual of 100
+    zero-start iterations + 0.1 %."""
+    import torch
+    from tigre_b200 import _native as N, projectors as P
+    from tigre_b200.algorithms._common import Problem
+    from tigre_b200.algorithms.krylov import cgls_device
+    from tigre_b200.algorithms.single_pass import fdk_device
+    from tigre_b200.utilities.phantom import random_ellipsoids
+    geo, ang = c5_geometry(), c5_angles()
+    img = random_ellipsoids((C5_VOX,) * 3, seed=0, device="cuda")
+    plan = N.get_plan(N.checked_geometry(geo, ang), img.device.index)
+    clean = P.ax(img, plan, "Siddon")
+    out = {"workload": C5_WORKLOAD}
+
+    def run(prob, x0, target):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        _, res, _ = cgls_device(prob, C5_MAX_ITERS, x0=x0, tol=target)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t
+        rel = np.asarray(res) / prob_bnorm(prob)
+        hit = np.nonzero(rel <= target)[0]
+        return {"s": round(dt, 4), "iters": int(hit[0]) + 1 if hit.size else len(rel), "reached": bool(hit.size),
+                "final_rel_residual": float(rel[-1])}
+
+    def prob_bnorm(prob):
+        return float(torch.linalg.vector_norm(prob.b.double()).item())
+
+    for variant in ("noiseless", "noisy"):
+        b = clean if variant == "noiseless" else torch.from_numpy(c5_noise(clean.cpu().numpy())).cuda()
+        prob = Problem(b, geo, ang)
+        cgls_device(prob, 3)                       # warm-up: plan, scratch, pools
+        if variant == "noiseless":
+            target, crit = C5_TOL, "||b - Ax|| / ||b|| <= 1e-3"
+        else:
+            _, res100, _ = cgls_device(prob, 100)
+            target = float(res100[-1] / prob_bnorm(prob)) * 1.001
+            crit = "||b - Ax|| / ||b|| <= 1.001 x its value after 100 zero-start iterations (%.5f)" % target
+        row = {"criterion": crit, "target": target, "zero": run(prob, None, target)}
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        f = fdk_device(prob).clamp_(min=0)
+        torch.cuda.synchronize()
+        t_fdk = time.perf_counter() - t
+        fr = run(prob, f, target)
+        fr["fdk_s"] = round(t_fdk, 4)
+        fr["s"] = round(fr["s"] + t_fdk, 4)
+        row["fdk"] = fr
+        out[variant] = row
+    return out
+
+
+def reference_cgls(T, ref_geo):
+    """The reference's own tigre.algorithms.cgls (krylov_subspace_algorithms.py:22-99) on the
+    same data, numpy in and out.  It has no tolerance stop: it runs a fixed number of
+    iterations, logging ||b - A x|| every iteration with an extra projection; the time to the
+    criterion is the run time up to the first iteration that meets it (iterations take equal
+    time), or the whole run when none does."""
+    from tigre_b200.utilities.phantom import random_ellipsoids
+    ang = c5_angles()
+    img = random_ellipsoids((C5_VOX,) * 3, seed=0).cpu().numpy()
+    clean = T.Ax(img, ref_geo, ang, "Siddon")
+    out = {"workload": C5_WORKLOAD}
+    for variant, niter in (("noiseless", 40), ("noisy", 40)):
+        b = clean if variant == "noiseless" else c5_noise(clean)
+        bnorm = float(np.linalg.norm(b.astype(np.float64)))
+        T.algorithms.cgls(b, ref_geo, ang, 2)      # warm-up
+        t = time.perf_counter()
+        _, l2 = T.algorithms.cgls(b, ref_geo, ang, niter, computel2=True)
+        dt = time.perf_counter() - t
+        rel = np.asarray(l2, dtype=np.float64).ravel() / bnorm
+        out[variant] = {"iters_run": niter, "s_run": round(dt, 3), "s_per_iter": round(dt / niter, 4),
+                        "rel_residual": [float(r) for r in rel[:: max(1, niter // 10)]]}
+        if variant == "noiseless":
+            hit = np.nonzero(rel <= C5_TOL)[0]
+            out[variant]["reached_1e-3"] = bool(hit.size)
+            if hit.size:
+                out[variant]["s_to_1e-3"] = round(dt * (int(hit[0]) + 1) / niter, 3)
+    return out
+
+
 def run_reference(args, rank):
+    """TIGRE's own package over its own CUDA build for sm_100a (baseline/_ref, made by
+    tests/dropin/build.py from the unmodified sources), through its public Python API:
+    tigre.Ax / tigre.Atb on numpy arrays, as a TIGRE user calls them."""
     if rank != 0:
         return
-    from oracle import ref
-    geo, ang = geometry(), angles()
-    if not ref.available():
-        print(json.dumps({"impl": "reference", "unavailable": "reference CUDA build (oracle/_ref) not present"}))
+    from oracle import reference_package as RP
+    if not RP.available("reference"):
+        print(json.dumps({"impl": "reference", "unavailable": "stock TIGRE build (baseline/_ref) not present"}))
         return
+    T = RP.load("reference")
+    geo, ang = RP.geometry_like(T, geometry()), angles()
     img = _phantom_host(0)
-    reps = args.warmup + args.steps
-    proj, t_ax = ref.ax(img, geo, ang, "Siddon", repeat=reps)
-    _, t_atb = ref.atb(proj, geo, ang, "matched", repeat=reps)
-    t_ax, t_atb = t_ax[args.warmup:], t_atb[args.warmup:]
+    for _ in range(max(1, args.warmup)):
+        proj = T.Ax(img, geo, ang, "Siddon")
+        T.Atb(proj, geo, ang, "matched")
+    t_ax, t_atb = [], []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        proj = T.Ax(img, geo, ang, "Siddon")
+        t_ax.append(time.perf_counter() - t)
+        t = time.perf_counter()
+        T.Atb(proj, geo, ang, "matched")
+        t_atb.append(time.perf_counter() - t)
     rays, upd = NA * NU * NV, NA * math.prod(NVOX)
     v = rays / statistics.median(t_ax) / 1e9
     va = upd / statistics.median(t_atb) / 1e9
@@ -240,8 +369,9 @@ def run_reference(args, rank):
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1e3 * (statistics.median(t_ax) + statistics.median(t_atb)), 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "reference": "TIGRE Common/CUDA built for sm_100a, host-pointer API "
-                                                      "siddon_ray_projection + voxel_backprojection2"},
+        "config": {"workload": WORKLOAD, "reference": "TIGRE's Python package with its Cython extensions and "
+                                                      "Common/CUDA built for sm_100a: tigre.Ax(Siddon) + "
+                                                      "tigre.Atb(matched) on pageable numpy arrays"},
         "atb": {"value": round(va, 4), "unit": "Gvox-upd/s"},
         "e2e": {"value": round(v, 4), "unit": "GRays/s", "atb_value": round(va, 4), "atb_unit": "Gvox-upd/s",
                 "h2d_bytes_per_step": b_in + b_out, "d2h_bytes_per_step": b_out + b_in},
@@ -249,18 +379,27 @@ def run_reference(args, rank):
                          "sample": "full workload; the reference has no CPU projector, its CUDA build runs on the GPU"},
     }
     if not args.no_ops:
-        # the reference's other projector kinds through the same host API (one untimed call first)
         ops = {}
-        _, t_int = ref.ax(img, geo, ang, "interpolated", repeat=2)
-        ops["ax_interpolated_f32"] = {"value": round(rays / t_int[-1] / 1e9, 4), "unit": "GRays/s",
-                                      "ms_per_call": round(1e3 * t_int[-1], 3)}
-        _, t_fdk = ref.atb(proj, geo, ang, "FDK", repeat=2)
-        ops["atb_fdk_f32"] = {"value": round(upd / t_fdk[-1] / 1e9, 4), "unit": "Gvox-upd/s",
-                              "ms_per_call": round(1e3 * t_fdk[-1], 3)}
-        _, t_tv = ref.pocs_tv(img, TV_ALPHA, TV_ITERS, repeat=2)
-        ops["tv_pocs_f32_e2e"] = {"value": round(math.prod(NVOX) * TV_ITERS / t_tv[-1] / 1e9, 4),
-                                  "unit": "Gvox-iter/s", "ms_per_call": round(1e3 * t_tv[-1], 3)}
+        T.Ax(img, geo, ang, "interpolated")
+        t = time.perf_counter()
+        T.Ax(img, geo, ang, "interpolated")
+        dt = time.perf_counter() - t
+        ops["ax_interpolated_f32"] = {"value": round(rays / dt / 1e9, 4), "unit": "GRays/s", "ms_per_call": round(1e3 * dt, 3)}
+        T.Atb(proj, geo, ang, "FDK")
+        t = time.perf_counter()
+        T.Atb(proj, geo, ang, "FDK")
+        dt = time.perf_counter() - t
+        ops["atb_fdk_f32"] = {"value": round(upd / dt / 1e9, 4), "unit": "Gvox-upd/s", "ms_per_call": round(1e3 * dt, 3)}
+        from _minTV import minTV
+        minTV(img, TV_ALPHA, TV_ITERS)
+        t = time.perf_counter()
+        minTV(img, TV_ALPHA, TV_ITERS)
+        dt = time.perf_counter() - t
+        ops["tv_pocs_f32_e2e"] = {"value": round(math.prod(NVOX) * TV_ITERS / dt / 1e9, 4), "unit": "Gvox-iter/s",
+                                  "ms_per_call": round(1e3 * dt, 3)}
         line["ops"] = ops
+    if not args.no_cgls:
+        line["cgls"] = reference_cgls(T, RP.geometry_like(T, c5_geometry()))
     print(json.dumps(line))
 
 
@@ -273,6 +412,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ops", action="store_true", help="skip the per-kind kernel timings")
+    ap.add_argument("--no-cgls", action="store_true", help="skip the CGLS time-to-residual measurement")
     ap.add_argument("--size", type=int, default=512, choices=[512, 256])
     ap.add_argument("--views", type=int, default=0)
     ap.add_argument("--cpu-configs", action="store_true",
@@ -350,12 +490,14 @@ def main():
         rpt = 8 if NV >= 512 else (4 if NV >= 256 else 2)   # rows per thread, as the launcher picks
         roof = {"kernel": "siddon_cells_kernel<float,float,%d>" % rpt, "bound": "hbm",
                 "achieved": alg / ax_launch / 1e9, "alg_bytes_per_launch": alg,
-                "traffic": _scaled_traffic("siddon", NA)}
+                "traffic": _scaled_traffic("siddon", NA), "traffic_source": TRAFFIC_SOURCE,
+                "binding": _binding("siddon", ax_launch)}
     else:
         alg = upd * 4 * 4 + math.prod(NVOX) * 4   # 4 bilinear taps per update + one volume write
         roof = {"kernel": "bp_tma_kernel<float,float,true,true>", "bound": "hbm",
                 "achieved": alg / atb_launch / 1e9, "alg_bytes_per_launch": alg,
-                "traffic": _scaled_traffic("bp", NA)}
+                "traffic": _scaled_traffic("bp", NA), "traffic_source": TRAFFIC_SOURCE,
+                "binding": _binding("bp", atb_launch)}
     roof.update({"peak": peak, "unit": "GB/s", "frac": roof["achieved"] / peak, "peak_source": peak_kind})
     for k in ("achieved", "frac"):
         roof[k] = round(roof[k], 4)
@@ -365,6 +507,10 @@ def main():
     e2e = None
     if not args.no_e2e and rank == 0:
         e2e = measure_e2e(vol, geo, ang, min(args.steps, 3))
+    cgls = None
+    if not args.no_cgls and rank == 0:
+        del bp
+        cgls = measure_cgls()
     if dist:
         dist.barrier()
     if rank == 0:
@@ -388,6 +534,8 @@ def main():
             line["ops"] = ops
         if e2e:
             line["e2e"] = e2e
+        if cgls:
+            line["cgls"] = cgls
         if not args.no_cpu:
             try:
                 line["cpu_baseline"] = cpu_baseline(geo, ang)
@@ -405,6 +553,39 @@ def main():
 # in L2; the backprojector reads each view's patches once per voxel block), so the figure is
 # reported only for that exact launch.
 TRAFFIC_720_VIEWS = {"siddon": 6644203008 + 2288307968, "bp": 17286047744 + 527202816}
+
+
+TRAFFIC_SOURCE = ("dram__bytes_read.sum + dram__bytes_write.sum of a single-pass ncu capture of the 720-view "
+                  "launch on B200 (profiles/launches_512cube_720views.txt), not measured in this run")
+
+# What binds each kernel, from its ncu --set full capture on 36 views of the same workload
+# (profiles/siddon_cells_512cube_36views.txt, profiles/bp_tma_matched_512cube_36views.txt): warp
+# instructions and shared-memory wavefronts per view of the launch.  The Siddon kernel's DRAM
+# traffic is 0.6 % of its algorithmic bytes: it is bound by instruction issue and on-chip load
+# latency; the backprojector reads its taps from shared memory: bound by shared wavefronts and issue.
+PROFILED = {"siddon": {"warp_inst_per_view": 6.127e9 / 36, "source": "profiles/siddon_cells_512cube_36views.txt"},
+            "bp": {"warp_inst_per_view": 3.120e9 / 36, "wavefronts_per_view": 7.603e8 / 36,
+                   "ideal_wavefronts_per_view": 512 ** 3 * 4 / 32,
+                   "source": "profiles/bp_tma_matched_512cube_36views.txt"}}
+
+
+def _binding(kind, launch_s):
+    """Fraction of the resource that binds the kernel: instruction issue (4 warp instructions per
+    SM per clock) for both, and for the backprojector shared-memory wavefronts (1 per SM per
+    clock), at the SM clock of the GPU's specification (the clocks key gives the measured one)."""
+    if NVOX != (512, 512, 512) or NU != 1024 or NV != 768:
+        return None
+    sms, hz = 148, 1.965e9
+    pr = PROFILED[kind]
+    out = {"issue_frac": round(pr["warp_inst_per_view"] * NA / launch_s / (sms * 4 * hz), 4),
+           "source": pr["source"] + " (counts per view, scaled to this launch)"}
+    if kind == "bp":
+        out["resource"] = "shared-memory wavefronts and instruction issue"
+        out["shared_wavefront_frac"] = round(pr["wavefronts_per_view"] * NA / launch_s / (sms * hz), 4)
+        out["shared_wavefront_floor_ms"] = round(1e3 * pr["ideal_wavefronts_per_view"] * NA / (sms * hz), 2)
+    else:
+        out["resource"] = "instruction issue and L1/L2 load latency (long-scoreboard stalls)"
+    return out
 
 
 def _scaled_traffic(kind, views):
@@ -484,12 +665,10 @@ def time_ops(P, plan, vol, proj, reps=3):
 
 
 def measure_e2e(vol, geo, ang, steps):
-    """Public host API: pinned numpy in, numpy out, copies inside the timed region."""
-    import torch
+    """Public host API: numpy in (ordinary pageable arrays, as TIGRE users pass them and as the
+    reference arm gets them), numpy out, copies inside the timed region."""
     import tigre_b200 as tigre
-    img = torch.empty(vol.shape, dtype=torch.float32, pin_memory=True)
-    img.copy_(vol)
-    img_np = img.numpy()
+    img_np = np.ascontiguousarray(vol.cpu().numpy())
     tigre.Ax(img_np, geo, ang, "Siddon")    # warm-up (plan, pools)
     ta, tb = [], []
     proj_np = None
@@ -497,22 +676,20 @@ def measure_e2e(vol, geo, ang, steps):
         t = time.perf_counter()
         proj_np = tigre.Ax(img_np, geo, ang, "Siddon")
         ta.append(time.perf_counter() - t)
-    pin = torch.empty(proj_np.shape, dtype=torch.float32, pin_memory=True)
-    pin.copy_(torch.from_numpy(proj_np))
-    pin_np = pin.numpy()
-    tigre.Atb(pin_np, geo, ang, "matched")
+    proj_in = np.array(proj_np)   # a pageable copy of the projections as the backprojection input
+    tigre.Atb(proj_in, geo, ang, "matched")
     for _ in range(steps):
         t = time.perf_counter()
-        tigre.Atb(pin_np, geo, ang, "matched")
+        tigre.Atb(proj_in, geo, ang, "matched")
         tb.append(time.perf_counter() - t)
     # the other two kinds through the same host API (one untimed call first, one timed)
     tigre.Ax(img_np, geo, ang, "interpolated")
     t = time.perf_counter()
     tigre.Ax(img_np, geo, ang, "interpolated")
     ti = time.perf_counter() - t
-    tigre.Atb(pin_np, geo, ang, "FDK")
+    tigre.Atb(proj_in, geo, ang, "FDK")
     t = time.perf_counter()
-    tigre.Atb(pin_np, geo, ang, "FDK")
+    tigre.Atb(proj_in, geo, ang, "FDK")
     tf = time.perf_counter() - t
     rays, upd = NA * NU * NV, NA * math.prod(NVOX)
     b_vol, b_proj = math.prod(NVOX) * 4, NA * NU * NV * 4

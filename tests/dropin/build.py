@@ -1,20 +1,23 @@
-"""Build TIGRE's own Python package on top of libtigre_b200.so (test infrastructure only).
+"""Build TIGRE's own Python package with its Cython extensions (test and bench infrastructure).
 
     python tests/dropin/build.py [--force]          # CPU only; needs the TIGRE source tree
 
-This is the drop-in that the C ABI promises, done the way a maintainer of TIGRE would do it:
-the reference's Python package (Python/tigre, copied unmodified into tests/dropin/_build/,
-which git ignores) gets its eight Cython extensions (top-level modules _Ax, _Atb, ..., beside
-the package, as the reference's setup.py installs them) compiled from the reference's own
-unmodified .pyx files, with the extension blocks of the reference's setup.py:347-509 except
-that the CUDA sources of the projectors and regularisers (Siddon_projection.cu,
-voxel_backprojection*.cu, GD_TV.cu, ...) are replaced by linking libtigre_b200.so, which
-exports the same C++ symbols (include/tigre_b200_compat.hpp).  The host-side helpers that the
-extensions compile in the reference build are kept from the TIGRE tree (GpuIds.cpp,
-gpuUtils.cu).  Nothing here runs at test time: tests/test_dropin_gpu.py imports the result.
+Two builds of the same unmodified package (Python/tigre, copied, never committed) and of its
+eight Cython extensions (top-level modules _Ax, _Atb, ..., beside the package, as the
+reference's setup.py installs them), compiled from the reference's own .pyx files with the
+extension blocks of its setup.py:347-509:
 
-The TIGRE tree is read in place from $TIGRE_REFERENCE (default /root/reference); without it this
-script does nothing.
+* backend "ours" -> tests/dropin/_build/: the drop-in that the C ABI promises.  The CUDA
+  sources of the projectors and regularisers (Siddon_projection.cu, voxel_backprojection*.cu,
+  GD_TV.cu, ...) are replaced by linking libtigre_b200.so, which exports the same C++
+  symbols (include/tigre_b200_compat.hpp).  tests/test_dropin_gpu.py imports it.
+* backend "reference" -> baseline/_ref/: the stock reference, every extension compiled with
+  its own CUDA sources for sm_100a (the flags of setup.py:32-36), as `pip install` would
+  build it on this GPU.  bench.py's reference arm imports it.
+
+Both keep the host-side helpers the extensions compile in the reference build (GpuIds.cpp,
+gpuUtils.cu, TIGRE_common.cpp, projection.cpp) from the TIGRE tree, which is read in place
+from $TIGRE_REFERENCE (default /root/reference); without it this script does nothing.
 """
 from __future__ import annotations
 
@@ -27,26 +30,29 @@ from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-OUT = os.path.join(HERE, "_build")
-PKG = os.path.join(OUT, "tigre")
-PYX_DIR = os.path.join(PKG, "utilities", "cuda_interface")
-OBJ = os.path.join(OUT, "obj")
+OUT = {"ours": os.path.join(HERE, "_build"), "reference": os.path.join(ROOT, "baseline", "_ref")}
 REFERENCE_ROOT = os.environ.get("TIGRE_REFERENCE", "/root/reference")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB_DIR = os.path.join(ROOT, "tigre_b200")
 
-# extension -> (pyx, host helpers of the TIGRE tree it compiles in the reference build,
-#               whether it links libtigre_b200.so); setup.py:347-509
+# extension -> (pyx, sources of the reference's Extension block, setup.py:347-509).  The
+# backend "ours" keeps the host helpers and links libtigre_b200.so instead of the rest.
+HOST_HELPERS = ("GpuIds.cpp", "gpuUtils.cu", "TIGRE_common.cpp", "projection.cpp")
 EXTENSIONS = {
-    "_Ax": ("_Ax.pyx", ["GpuIds.cpp"], True),
-    "_Atb": ("_Atb.pyx", ["GpuIds.cpp", "gpuUtils.cu"], True),
-    "_tv_proximal": ("_tv_proximal.pyx", ["GpuIds.cpp", "gpuUtils.cu"], True),
-    "_minTV": ("_minTV.pyx", ["GpuIds.cpp", "gpuUtils.cu"], True),
-    "_minPICCS": ("_minPICCS.pyx", ["GpuIds.cpp", "gpuUtils.cu"], True),
-    "_AwminTV": ("_AwminTV.pyx", ["GpuIds.cpp", "gpuUtils.cu"], True),
-    "_gpuUtils": ("_gpuUtils.pyx", ["gpuUtils.cu"], False),
-    "_RandomNumberGenerator": ("_randomNumberGenerator.pyx", ["GpuIds.cpp", "gpuUtils.cu"], True),
+    "_Ax": ("_Ax.pyx", ["projection.cpp", "TIGRE_common.cpp", "Siddon_projection.cu",
+                        "Siddon_projection_parallel.cu", "ray_interpolated_projection.cu",
+                        "ray_interpolated_projection_parallel.cu", "GpuIds.cpp"]),
+    "_Atb": ("_Atb.pyx", ["TIGRE_common.cpp", "voxel_backprojection.cu", "voxel_backprojection2.cu",
+                          "voxel_backprojection_parallel.cu", "GpuIds.cpp", "gpuUtils.cu"]),
+    "_tv_proximal": ("_tv_proximal.pyx", ["TIGRE_common.cpp", "tv_proximal.cu", "GpuIds.cpp", "gpuUtils.cu"]),
+    "_minTV": ("_minTV.pyx", ["TIGRE_common.cpp", "GD_TV.cu", "GpuIds.cpp", "gpuUtils.cu"]),
+    "_minPICCS": ("_minPICCS.pyx", ["TIGRE_common.cpp", "PICCS.cu", "GpuIds.cpp", "gpuUtils.cu"]),
+    "_AwminTV": ("_AwminTV.pyx", ["TIGRE_common.cpp", "GD_AwTV.cu", "GpuIds.cpp", "gpuUtils.cu"]),
+    "_gpuUtils": ("_gpuUtils.pyx", ["gpuUtils.cu"]),
+    "_RandomNumberGenerator": ("_randomNumberGenerator.pyx", ["TIGRE_common.cpp", "RandomNumberGenerator.cu",
+                                                             "GpuIds.cpp", "gpuUtils.cu"]),
 }
 
 
@@ -68,51 +74,67 @@ def available():
     return os.path.isdir(os.path.join(REFERENCE_ROOT, "Python", "tigre"))
 
 
-def build(force: bool = False) -> list[str]:
+def _sources(backend, srcs):
+    if backend == "ours":
+        return [s for s in srcs if s in HOST_HELPERS and s not in ("TIGRE_common.cpp", "projection.cpp")]
+    return list(srcs)
+
+
+def build(backend: str = "ours", force: bool = False) -> list[str]:
     """Returns the built extension paths ([] when the TIGRE tree is absent)."""
     if not available():
         return []
     import numpy as np
+    out = OUT[backend]
+    pkg = os.path.join(out, "tigre")
+    pyx_dir = os.path.join(pkg, "utilities", "cuda_interface")
+    obj_dir = os.path.join(out, "obj")
     cuda_src = os.path.join(REFERENCE_ROOT, "Common", "CUDA")
-    if force and os.path.isdir(PKG):
-        shutil.rmtree(PKG)
-    if not os.path.isdir(PKG):
-        shutil.copytree(os.path.join(REFERENCE_ROOT, "Python", "tigre"), PKG,
+    if force and os.path.isdir(pkg):
+        shutil.rmtree(pkg)
+    if not os.path.isdir(pkg):
+        shutil.copytree(os.path.join(REFERENCE_ROOT, "Python", "tigre"), pkg,
                         ignore=shutil.ignore_patterns("*.so", "__pycache__", "*.c", "*.cpp"))
-    os.makedirs(OBJ, exist_ok=True)
+    os.makedirs(obj_dir, exist_ok=True)
     suffix = sysconfig.get_config_var("EXT_SUFFIX")
     inc = ["-I" + sysconfig.get_paths()["include"], "-I" + np.get_include(), "-I" + os.path.join(CUDA, "include"),
            "-I" + cuda_src]
     defs = ["-DIS_FOR_PYTIGRE", "-DNPY_NO_DEPRECATED_API=NPY_1_7_API_VERSION"]
-    # host helpers, once
-    helpers = {}
-    for f in ("GpuIds.cpp", "gpuUtils.cu"):
+    # objects of the TIGRE sources, once each
+    needed = sorted({f for _, srcs in EXTENSIONS.values() for f in _sources(backend, srcs)})
+    objs = {}
+
+    def compile_one(f):
         src = os.path.join(cuda_src, f)
-        obj = os.path.join(OBJ, f.replace(".", "_") + ".o")
+        obj = os.path.join(obj_dir, f.replace(".", "_") + ".o")
         if force or _stale(obj, [src]):
             if f.endswith(".cu"):
-                _run([NVCC, "-O2", "-Xcompiler", "-fPIC", *defs, *inc, "-c", src, "-o", obj])
+                # setup.py:32-36: per-thread default stream; device code for this GPU only
+                _run([NVCC, *ARCH, "-O3", "--default-stream=per-thread", "-Xcompiler", "-fPIC", *defs, *inc,
+                      "-c", src, "-o", obj])
             else:
                 _run(["g++", "-O2", "-fPIC", "-std=c++17", *defs, *inc, "-c", src, "-o", obj])
-        helpers[f] = obj
+        return f, obj
+
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        objs.update(dict(ex.map(compile_one, needed)))
     lib = os.path.join(LIB_DIR, "libtigre_b200.so")
-    # the extensions are top-level modules (setup.py names them "_Ax", ...; tigre/utilities/Ax.py
-    # imports "from _Ax import _Ax_ext"), so they sit in tests/dropin/_build, three levels below
-    # the repository
-    rpath = "$ORIGIN/../../../tigre_b200"
+    # the extensions sit three levels below the repository (tests/dropin/_build, baseline/_ref)
+    rpath = "$ORIGIN/../../../tigre_b200" if backend == "ours" else None
 
     def one(name):
-        pyx_name, extra, link_ours = EXTENSIONS[name]
-        pyx = os.path.join(PYX_DIR, pyx_name)
-        cpp = os.path.join(OBJ, name + ".cpp")
-        so = os.path.join(OUT, name + suffix)
-        deps = [pyx] + [helpers[e] for e in extra] + ([lib] if link_ours else [])
+        pyx_name, srcs = EXTENSIONS[name]
+        mine = [objs[f] for f in _sources(backend, srcs)]
+        link_ours = backend == "ours" and name != "_gpuUtils"
+        pyx = os.path.join(pyx_dir, pyx_name)
+        cpp = os.path.join(obj_dir, name + ".cpp")
+        so = os.path.join(out, name + suffix)
+        deps = [pyx] + mine + ([lib] if link_ours else [])
         if not (force or _stale(so, deps)):
             return so
-        _run([sys.executable, "-m", "cython", "--cplus", "-3", "--module-name", name, "-I", OUT, pyx, "-o", cpp])
-        cmd = ["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-w", *defs, *inc, cpp,
-               *[helpers[e] for e in extra], "-o", so, "-L" + os.path.join(CUDA, "lib64"), "-lcudart",
-               "-Wl,-rpath," + os.path.join(CUDA, "lib64")]
+        _run([sys.executable, "-m", "cython", "--cplus", "-3", "--module-name", name, "-I", out, pyx, "-o", cpp])
+        cmd = ["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-w", *defs, *inc, cpp, *mine, "-o", so,
+               "-L" + os.path.join(CUDA, "lib64"), "-lcudart", "-Wl,-rpath," + os.path.join(CUDA, "lib64")]
         if link_ours:
             cmd += ["-L" + LIB_DIR, "-ltigre_b200", "-Wl,-rpath," + rpath]
         _run(cmd)
@@ -123,5 +145,6 @@ def build(force: bool = False) -> list[str]:
 
 
 if __name__ == "__main__":
-    for p in build(force="--force" in sys.argv):
-        print(p)
+    for b in ("ours", "reference"):
+        for p in build(b, force="--force" in sys.argv):
+            print(p)

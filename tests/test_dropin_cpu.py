@@ -2,9 +2,7 @@
 without a GPU: every call reports the missing device through the reference's own error
 path instead of exiting the process, and the void regulariser entry points fill their
 output with NaN rather than return uninitialised memory."""
-import glob
 import os
-import sys
 
 import numpy as np
 import pytest
@@ -19,14 +17,10 @@ pytestmark = pytest.mark.skipif(has_gpu(), reason="checks the no-device error pa
 
 @pytest.fixture(scope="module")
 def T():
-    if not glob.glob(os.path.join(DROPIN, "_Ax*.so")):
+    from oracle import reference_package as RP
+    if not RP.available("ours"):
         pytest.skip("drop-in build absent (tests/dropin/build.py needs the TIGRE source tree)")
-    from tests.dropin import stub
-    stub.install()
-    if DROPIN not in sys.path:
-        sys.path.insert(0, DROPIN)
-    import tigre
-    return tigre
+    return RP.load("ours")
 
 
 def test_reference_calls_report_errors_instead_of_exiting(T):

@@ -8,9 +8,7 @@ public calls -- tigre.Ax, tigre.Atb, minTV, tigre.algorithms.cgls -- are checked
 FP64 oracle (bar 1e-5 relative for single operators; CGLS, whose vector algebra the reference
 does in float32 numpy, 2e-4 on the iterate).
 """
-import glob
 import os
-import sys
 
 import numpy as np
 import pytest
@@ -27,27 +25,15 @@ DROPIN = os.path.join(HERE, "dropin", "_build")
 
 @pytest.fixture(scope="module")
 def T():
-    if not glob.glob(os.path.join(DROPIN, "_Ax*.so")) or not os.path.isdir(os.path.join(DROPIN, "tigre")):
+    from oracle import reference_package as RP
+    if not RP.available("ours"):
         pytest.skip("drop-in build absent (tests/dropin/build.py needs the TIGRE source tree)")
-    from tests.dropin import stub
-    stub.install()
-    if DROPIN not in sys.path:
-        sys.path.insert(0, DROPIN)
-    import tigre
-    assert os.path.dirname(tigre.__file__) == os.path.join(DROPIN, "tigre"), tigre.__file__
-    import tigre.algorithms  # noqa: F401
-    return tigre
+    return RP.load("ours")
 
 
 def _ref_geometry(T, ours):
-    """The reference's own geometry object with the attributes of one of ours."""
-    g = T.geometry()
-    for name in ("mode", "nVoxel", "sVoxel", "dVoxel", "nDetector", "sDetector", "dDetector", "DSO", "DSD",
-                 "offOrigin", "offDetector", "rotDetector", "accuracy", "COR"):
-        if hasattr(ours, name):
-            v = getattr(ours, name)
-            setattr(g, name, np.array(v) if isinstance(v, np.ndarray) else v)
-    return g
+    from oracle import reference_package as RP
+    return RP.geometry_like(T, ours)
 
 
 def _maps():

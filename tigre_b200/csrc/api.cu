@@ -362,12 +362,11 @@ constexpr unsigned kStageThreads = 8;
 
 // which (bit mask, option TIGRE_OPT_HOST_STAGING, default kStageDefault): 1 uploads of a volume, 2 downloads
 // of a volume, 4 the backprojector's projection-chunk uploads, 8 the backprojector's volume
-// download.  Measured at 512^3 on B200 (host call, best of three): the POCS-TV call takes
-// 175 ms direct, 146 ms with staged uploads and 62 ms with staged uploads and downloads; the
-// Siddon Ax call 260 ms direct and 231 ms with its volume upload staged; the matched Atb call
-// 97 ms direct but 104-108 ms with its chunk uploads or its volume download staged (its uploads
-// already overlap the kernels), so the backprojector keeps the driver's path.
-constexpr int kStageDefault = 3;
+// download.  Page-locked caller buffers always take the direct path.  Measured at 512^3 on B200
+// (host call): the POCS-TV call takes 175 ms direct, 146 ms with staged uploads and 62 ms with
+// staged uploads and downloads; the Siddon Ax call 260 ms direct and 231 ms with its volume upload
+// staged; the matched Atb call on pageable projections 229 ms through the driver's pageable path.
+constexpr int kStageDefault = 1 | 2 | 4 | 8;
 bool staging_on(int which) {
     const long long o = option(TIGRE_OPT_HOST_STAGING);
     const long long mask = o >= 0 ? o : kStageDefault;
