@@ -226,6 +226,9 @@ void tigre_release_cache(void);
 #define TIGRE_OPT_BP_SKIP_COPY 6     /* -1 off; else the staged backprojector issues no copy for this view index
                                         of every launch, so the wait for it runs out: the kernel then sets the
                                         plan status and the call returns TIGRE_ERR_CUDA (failure-detection test) */
+#define TIGRE_OPT_INTERP_TEXTURE 7    /* 0 exact trilinear (default); 1 the interpolated projector samples through
+                                        the texture unit's linear filter (8-bit weights, ~2^-9 relative per
+                                        sample, as the reference's texture path) */
 long long tigre_set_option(int option, long long value);
 long long tigre_get_option(int option);
 

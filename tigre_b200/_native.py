@@ -25,6 +25,7 @@ PLAN_PARALLEL = 1
 STATUS_WAIT_EXPIRED, STATUS_RAY_DROPPED = 1, 2
 # library options (tigre_set_option)
 OPT_SIDDON_KERNEL, OPT_BP_BOX, OPT_BP_KERNEL, OPT_HOST_CHUNK_VIEWS, OPT_HOST_STAGING, OPT_BP_SKIP_COPY = 1, 2, 3, 4, 5, 6
+OPT_INTERP_TEXTURE = 7
 
 _FP = C.POINTER(C.c_float)
 

@@ -51,7 +51,8 @@ void layouts_needed(const TigrePlan* p, int a0, int a1, bool& l0, bool& l1) {
 // views and reused by every launch over sub-ranges of it (the host pipeline projects in view
 // chunks).  Lives in the plan's scratch until the next plan_scratch call.
 struct AxWork {
-    enum Mode { CELLS, COLUMNS, GENERAL, INTERP } mode = GENERAL;
+    enum Mode { CELLS, COLUMNS, GENERAL, INTERP, INTERP_TEX } mode = GENERAL;
+    unsigned long long tex = 0;   // INTERP_TEX: texture object over the plan's 3-D array
     const void* vx = nullptr;
     const void* vy = nullptr;
     const void* qx = nullptr;
@@ -98,6 +99,19 @@ int ax_prepare(TigrePlan* plan, const void* d_vol, int vdt, int projector, int a
             w->vy = s;
         }
         return TIGRE_SUCCESS;
+    }
+    if (projector == TIGRE_PROJ_INTERPOLATED && option(TIGRE_OPT_INTERP_TEXTURE) && d.accuracy <= 1.0) {
+        // hardware trilinear: the volume goes into the plan's FP32 3-D array (16-bit storage is
+        // widened first, exactly)
+        const float* vf = (const float*)d_vol;
+        if (vdt != TIGRE_F32) {
+            float* s = (float*)plan_scratch(plan, (size_t)d.nX * d.nY * d.nZ * sizeof(float), st, &rc);
+            if (rc) return rc;
+            if ((rc = tigre_convert(d_vol, vdt, s, TIGRE_F32, (long)d.nX * d.nY * d.nZ, st))) return rc;
+            vf = s;
+        }
+        w->mode = AxWork::INTERP_TEX;
+        return interp_texture(plan, vf, st, &w->tex);
     }
     if (projector == TIGRE_PROJ_INTERPOLATED) {
         // zero-padded copies (1 before, 2 after), x- and/or y-fastest; trilinear sampling reads
@@ -154,6 +168,7 @@ int ax_launch(TigrePlan* plan, const AxWork& w, void* d_proj, int pdt, int a0, i
         case AxWork::CELLS: return launch_siddon_cells(plan, w.vx, w.vdt, d_proj, pdt, a0, a1, st);
         case AxWork::COLUMNS: return launch_siddon_columns(plan, w.vx, w.vdt, d_proj, pdt, a0, a1, st);
         case AxWork::GENERAL: return launch_siddon(plan, w.vx, w.vy, w.vdt, d_proj, pdt, a0, a1, st);
+        case AxWork::INTERP_TEX: return launch_interp_tex(plan, w.tex, d_proj, pdt, a0, a1, st);
         default: return launch_interp(plan, w.vx, w.vy, w.qx, w.qy, w.vdt, d_proj, pdt, a0, a1, st);
     }
 }

@@ -247,6 +247,63 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs p) {
     ((TP*)p.proj)[oidx] = from_f32<TP>(sum * (float)dl);
 }
 
+// Hardware-texture variant (TIGRE_OPT_INTERP_TEXTURE): the same samples, each one tex3D fetch
+// with the texture unit's linear filter from an FP32 3-D array, border 0, texel centres at +0.5
+// -- the reference's own sampling (ray_interpolated_projection.cu:193-199, texture set up at
+// :549-603).  The filter weights are the texture unit's 8-bit fractions, so results differ
+// from the exact trilinear kernel by up to ~2^-9 relative per sample.
+template <typename TP>
+__global__ void __launch_bounds__(256) interp_tex_kernel(InterpArgs p, cudaTextureObject_t tex) {
+    const int u0 = blockIdx.x * 32 + threadIdx.x;
+    const int la = blockIdx.y;
+    const int v = blockIdx.z * blockDim.y + threadIdx.y;
+    if (v >= p.nV || u0 >= p.nU) return;
+    const int u = u0;
+    const FrameInterp& F = p.frames[p.a0 + la];
+    double s[3], vec[3];
+    const double length = interp_setup(p, F, u, v, s, vec);
+    double lo = F.first_sample, hi = length;
+    const int n[3] = {p.nX, p.nY, p.nZ};
+    bool empty = false;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (vec[k] != 0.0) {
+            const double ta = (-1.0 - s[k]) / vec[k], tb = ((double)n[k] - s[k]) / vec[k];
+            lo = fmax(lo, floor(fmin(ta, tb)));
+            hi = fmin(hi, ceil(fmax(ta, tb)));
+        } else if (s[k] <= -1.0 || s[k] >= (double)n[k]) {
+            empty = true;
+        }
+    }
+    const size_t oidx = ((size_t)la * p.nV + v) * (size_t)p.nU + u;
+    if (empty || lo > hi) {
+        ((TP*)p.proj)[oidx] = from_f32<TP>(0.f);
+        return;
+    }
+    const int first = (int)lo;
+    const int nsamp = (int)hi - first + 1;
+    // texture coordinates of the first sample (texel i spans [i, i+1), centre i + 0.5)
+    const float qx = (float)(fma(vec[0], (double)first, s[0]) + 0.5);
+    const float qy = (float)(fma(vec[1], (double)first, s[1]) + 0.5);
+    const float qz = (float)(fma(vec[2], (double)first, s[2]) + 0.5);
+    const float vx = (float)vec[0], vy = (float)vec[1], vz = (float)vec[2];
+    float sa = 0.f, sb = 0.f;
+    int k = 0;
+#pragma unroll 2
+    for (; k + 1 < nsamp; k += 2) {
+        const float ka = (float)k, kb = (float)(k + 1);
+        sa += tex3D<float>(tex, fmaf(ka, vx, qx), fmaf(ka, vy, qy), fmaf(ka, vz, qz));
+        sb += tex3D<float>(tex, fmaf(kb, vx, qx), fmaf(kb, vy, qy), fmaf(kb, vz, qz));
+    }
+    if (k < nsamp) {
+        const float ka = (float)k;
+        sa += tex3D<float>(tex, fmaf(ka, vx, qx), fmaf(ka, vy, qy), fmaf(ka, vz, qz));
+    }
+    const double dl = sqrt(vec[0] * p.dVX * vec[0] * p.dVX + vec[1] * p.dVY * vec[1] * p.dVY +
+                           vec[2] * p.dVZ * vec[2] * p.dVZ);
+    ((TP*)p.proj)[oidx] = from_f32<TP>((sa + sb) * (float)dl);
+}
+
 template <typename TV, typename TP>
 void launch_typed(const InterpArgs& a, bool nearest, dim3 grid, dim3 block, cudaStream_t st) {
     if (nearest) interp_kernel<TV, TP, true><<<grid, block, 0, st>>>(a);
@@ -301,6 +358,62 @@ int launch_interp(TigrePlan* P, const void* vol_x, const void* vol_y, const void
         else if (vdt == TIGRE_F32 && pdt == TIGRE_BF16) launch_typed<float, __nv_bfloat16>(ac, nearest, grid, block, st);
         else if (vdt == TIGRE_F32 && pdt == TIGRE_F16) launch_typed<float, __half>(ac, nearest, grid, block, st);
         else return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype pair for interpolated projection");
+        TIGRE_LAUNCHED();
+    }
+    return TIGRE_SUCCESS;
+}
+
+}  // namespace tigre
+
+namespace tigre {
+
+// The plan's FP32 3-D array and linear-filter texture object, sized to the volume (made once
+// per plan, reused by every call), filled from d_vol (FP32, (nZ, nY, nX)) on stream st.
+int interp_texture(TigrePlan* P, const float* d_vol, cudaStream_t st, unsigned long long* tex_out) {
+    const Dims& d = P->d;
+    if (!P->tex_array) {
+        cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+        TIGRE_CUDA(cudaMalloc3DArray(&P->tex_array, &ch, make_cudaExtent(d.nX, d.nY, d.nZ)));
+        cudaResourceDesc rd{};
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = P->tex_array;
+        cudaTextureDesc td{};
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        cudaTextureObject_t t = 0;
+        TIGRE_CUDA(cudaCreateTextureObject(&t, &rd, &td, nullptr));
+        P->tex_obj = t;
+    }
+    cudaMemcpy3DParms cp{};
+    cp.srcPtr = make_cudaPitchedPtr(const_cast<float*>(d_vol), (size_t)d.nX * sizeof(float), d.nX, d.nY);
+    cp.dstArray = P->tex_array;
+    cp.extent = make_cudaExtent(d.nX, d.nY, d.nZ);
+    cp.kind = cudaMemcpyDeviceToDevice;
+    TIGRE_CUDA(cudaMemcpy3DAsync(&cp, st));
+    *tex_out = (unsigned long long)P->tex_obj;
+    return TIGRE_SUCCESS;
+}
+
+int launch_interp_tex(TigrePlan* P, unsigned long long tex, void* proj, int pdt, int a0, int a1, cudaStream_t st) {
+    InterpArgs a{};
+    a.frames = P->d_interp;
+    a.nX = P->d.nX; a.nY = P->d.nY; a.nZ = P->d.nZ; a.nU = P->d.nU; a.nV = P->d.nV;
+    a.dVX = P->d.dVX; a.dVY = P->d.dVY; a.dVZ = P->d.dVZ; a.acc = P->d.accuracy;
+    a.parallel = P->parallel ? 1 : 0;
+    const int rows = 8;
+    dim3 block(32, rows);
+    dim3 grid((P->d.nU + 31) / 32, 1, (P->d.nV + rows - 1) / rows);
+    const int na = a1 - a0;
+    for (int c = 0; c < na; c += 65535) {
+        InterpArgs ac = a;
+        ac.a0 = a0 + c;
+        ac.proj = (char*)proj + (size_t)c * P->d.nU * P->d.nV * dtype_size(pdt);
+        grid.y = std::min(65535, na - c);
+        if (pdt == TIGRE_F32) interp_tex_kernel<float><<<grid, block, 0, st>>>(ac, (cudaTextureObject_t)tex);
+        else if (pdt == TIGRE_BF16) interp_tex_kernel<__nv_bfloat16><<<grid, block, 0, st>>>(ac, (cudaTextureObject_t)tex);
+        else interp_tex_kernel<__half><<<grid, block, 0, st>>>(ac, (cudaTextureObject_t)tex);
         TIGRE_LAUNCHED();
     }
     return TIGRE_SUCCESS;

@@ -36,9 +36,10 @@ void note_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_o
 
 // ---- library options (tigre_set_option) ----
 namespace {
-constexpr int kNumOptions = 7;
-// defaults: SIDDON_KERNEL 0, BP_BOX 0, BP_KERNEL 0, HOST_CHUNK_VIEWS 0, HOST_STAGING -1, BP_SKIP_COPY -1
-std::atomic<long long> g_options[kNumOptions] = {{0}, {0}, {0}, {0}, {0}, {-1}, {-1}};
+constexpr int kNumOptions = 8;
+// defaults: SIDDON_KERNEL 0, BP_BOX 0, BP_KERNEL 0, HOST_CHUNK_VIEWS 0, HOST_STAGING -1, BP_SKIP_COPY -1,
+// INTERP_TEXTURE 0
+std::atomic<long long> g_options[kNumOptions] = {{0}, {0}, {0}, {0}, {0}, {-1}, {-1}, {0}};
 }  // namespace
 
 long long option(int key) {
@@ -663,6 +664,8 @@ void tigre_plan_destroy(TigrePlan* p) {
     cudaFree(p->d_bp);
     cudaFree(p->d_bpk);
     cudaFree(p->d_status);
+    if (p->tex_obj) cudaDestroyTextureObject((cudaTextureObject_t)p->tex_obj);
+    if (p->tex_array) cudaFreeArray(p->tex_array);
     cudaSetDevice(prev);
     delete p;
 }

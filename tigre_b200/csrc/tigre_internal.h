@@ -131,6 +131,9 @@ struct TigrePlan {
     int bp_box_u = 0, bp_box_v = 0;   // TMA patch box of the staged backprojector (0: not usable)
     int bp_box_u16 = 0;               // box width for 16-bit projections
     int* d_status = nullptr;          // kernel error word (bounded waits that expired)
+    // hardware-texture interpolated projector (TIGRE_OPT_INTERP_TEXTURE): FP32 3-D array + texture
+    cudaArray_t tex_array = nullptr;
+    unsigned long long tex_obj = 0;
     // growable stream-ordered scratch arena
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -166,6 +169,8 @@ int launch_siddon_columns(TigrePlan* p, const void* vol_z, int vdt, void* proj, 
                           cudaStream_t st);
 int launch_interp(TigrePlan* p, const void* vol_x, const void* vol_y, const void* quad_x, const void* quad_y, int vdt,
                   void* proj, int pdt, int a0, int a1, cudaStream_t st);
+int interp_texture(TigrePlan* p, const float* d_vol, cudaStream_t st, unsigned long long* tex_out);
+int launch_interp_tex(TigrePlan* p, unsigned long long tex, void* proj, int pdt, int a0, int a1, cudaStream_t st);
 int launch_backproject(TigrePlan* p, const void* proj_pad, int pdt, void* vol, int vdt, int matched, int a0, int a1,
                        int accumulate, cudaStream_t st);
 
