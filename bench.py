@@ -320,7 +320,7 @@ def reference_cgls(T, ref_geo):
     time), or the whole run when none does."""
     from tigre_b200.utilities.phantom import random_ellipsoids
     ang = c5_angles()
-    img = random_ellipsoids((C5_VOX,) * 3, seed=0).cpu().numpy()
+    img = np.asarray(random_ellipsoids((C5_VOX,) * 3, seed=0), dtype=np.float32)
     clean = T.Ax(img, ref_geo, ang, "Siddon")
     out = {"workload": C5_WORKLOAD}
     for variant, niter in (("noiseless", 40), ("noisy", 40)):

@@ -297,10 +297,18 @@ int tigre_philox4x32(unsigned int* d_out, long long nblocks, unsigned long long 
  * channel minor), zero padding 1, FP32 accumulation on the tensor cores.  d_col: scratch of
  * tigre_conv3d_col_elems(D, H, W, Cin) BF16 elements (d_dcol: as many floats). */
 long long tigre_conv3d_col_elems(long D, long H, long W, long C);
-/* Forward path of tigre_conv3d_fwd when Cin % 8 == 0 and Cout % 16 == 0: 0 the warp-level
- * implicit GEMM, 1 the tcgen05 implicit GEMM (TMEM accumulator), 2 (default) tcgen05 for narrow
- * layers (Cin <= 16 or Cout == 16) and the warp-level kernel otherwise.  Returns the old mode. */
+/* Forward path of tigre_conv3d_fwd (and of the data gradient): 3 (default) the tcgen05 halo-tile
+ * kernel -- one TMA load of a zero-padded input tile per 16 input channels, the 27 taps as
+ * shifted shared-memory operand descriptors, TMEM accumulators -- wherever Cin % 16 == 0,
+ * Cout % 16 == 0 (<= 192), W % 8 == 0 and H % 16 == 0, else mode 2; when Cin % 8 == 0 and
+ * Cout % 16 == 0: 0 the warp-level implicit GEMM, 1 the tcgen05 implicit GEMM with per-step
+ * gathers, 2 that kernel for narrow layers (Cin <= 16 or Cout == 16) and the warp-level one
+ * otherwise.  Returns the old mode. */
 int tigre_conv3d_set_tcgen05(int mode);
+/* Synchronises the current device and returns the tensor-core convolution kernels' status word
+ * (0 ok; TIGRE_STATUS_WAIT_EXPIRED: a bounded wait ran out and that output tile was not
+ * written); reset != 0 clears it.  -1 if it cannot be read. */
+int tigre_conv3d_status(int reset);
 int tigre_conv3d_fwd(const void* d_x, const void* d_w, const float* d_bias, void* d_y_bf16, float* d_y_f32, long D,
                      long H, long W, long Cin, long Cout, int relu, void* d_col, void* stream);
 int tigre_conv3d_bwd_data(const void* d_dy, const void* d_w, float* d_dx, long D, long H, long W, long Cin, long Cout,

@@ -23,8 +23,12 @@ def _ref_weights(w, cin, cout):
                                             ((4, 9, 6), 48, 1),
                                             # tcgen05 path: Cin % 8 == 0 and Cout % 16 == 0, N tiles 16..128
                                             ((8, 6, 10), 16, 16), ((7, 9, 11), 8, 32), ((9, 8, 7), 48, 48),
-                                            ((6, 6, 6), 24, 64), ((5, 7, 9), 16, 128), ((3, 4, 5), 64, 192)])
-@pytest.mark.parametrize("tcgen05", [0, 1])
+                                            ((6, 6, 6), 24, 64), ((5, 7, 9), 16, 128), ((3, 4, 5), 64, 192),
+                                            # halo-tile kernel: Cin % 16 == 0, W % 8 == 0, H % 16 == 0
+                                            ((4, 16, 8), 16, 16), ((8, 32, 16), 32, 32), ((6, 16, 24), 48, 16),
+                                            ((4, 16, 8), 16, 64), ((2, 16, 8), 64, 128), ((2, 16, 16), 32, 192),
+                                            ((5, 16, 8), 96, 32)])
+@pytest.mark.parametrize("tcgen05", [0, 1, 3])
 def test_conv3d_matches_torch_fp32(shape, cin, cout, tcgen05):
     import torch
     import torch.nn.functional as F
@@ -63,11 +67,32 @@ def test_conv3d_matches_torch_fp32(shape, cin, cout, tcgen05):
     N.check(L.tigre_conv3d_bwd_data(p(dyd), p(wd), p(dx), D, H, W, cin, cout, p(dcol), None), "data")
     N.check(L.tigre_conv3d_bwd_weight(p(xd), p(dyd), p(dw), D, H, W, cin, cout, p(col), None), "weight")
     torch.cuda.synchronize()
+    assert L.tigre_conv3d_status(1) == 0
     for got, ref, name in ((y, y_ref, "y"), (dx, dx_ref, "dx"), (dw, dw_ref, "dw")):
         got = got.cpu().numpy()
         # same BF16 operands, FP32 sums in another order (tensor-core accumulation): 2e-4 of the max
         err = np.max(np.abs(got - ref)) / max(np.max(np.abs(ref)), 1e-30)
         assert err <= 2e-4, (name, err)
+
+
+def test_conv3d_weight_gradient_is_deterministic():
+    """The weight gradient sums its voxel splits in a fixed order: repeated calls give the same
+    bits."""
+    import torch
+    from tigre_b200 import _native as N
+    L = N.lib()
+    D, H, W, cin, cout = 16, 32, 32, 16, 16
+    g = torch.Generator("cuda").manual_seed(5)
+    x = torch.randn((D, H, W, cin), device="cuda", generator=g).to(torch.bfloat16)
+    dy = torch.randn((D, H, W, cout), device="cuda", generator=g).to(torch.bfloat16)
+    col = torch.empty(int(L.tigre_conv3d_col_elems(D, H, W, cin)), dtype=torch.bfloat16, device="cuda")
+    p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    out = []
+    for _ in range(3):
+        dw = torch.zeros((cout, 27 * cin), dtype=torch.float32, device="cuda")
+        N.check(L.tigre_conv3d_bwd_weight(p(x), p(dy), p(dw), D, H, W, cin, cout, p(col), None), "weight")
+        out.append(dw.cpu())
+    assert torch.equal(out[0], out[1]) and torch.equal(out[0], out[2])
 
 
 def test_conv_autograd_matches_torch_fp32():

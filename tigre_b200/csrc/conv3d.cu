@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <mutex>
 
 #include "tigre_internal.h"
 
@@ -90,6 +91,10 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(const __nv_bfloat16* __r
         const int gi = m0 + i, gj = n0 + j;
         if (gi >= M || gj >= N) continue;
         float v = sC[i][j];
+        if (atomic == 2) {   // split-K partial: slice blockIdx.z of M x N
+            Cf[(size_t)blockIdx.z * M * ldc + (size_t)gi * ldc + gj] = v;
+            continue;
+        }
         if (atomic) {
             atomicAdd(Cf + (size_t)gi * ldc + gj, v);
             continue;
@@ -98,6 +103,15 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(const __nv_bfloat16* __r
         if (relu) v = fmaxf(v, 0.f);
         if (Cf) Cf[(size_t)gi * ldc + gj] = v;
         if (Cb) Cb[(size_t)gi * ldc + gj] = __float2bfloat16(v);
+    }
+}
+
+// dst[i] += sum over s < splits of ws[s * n + i], in order of s
+__global__ void reduce_slices_kernel(const float* __restrict__ ws, float* __restrict__ dst, long n, long splits) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        float acc = dst[i];
+        for (long s = 0; s < splits; ++s) acc += ws[s * n + i];
+        dst[i] = acc;
     }
 }
 
@@ -489,16 +503,46 @@ int grid_for_conv(long n) { return (int)std::min<long>((n + 255) / 256, 148L * 3
 
 using namespace tigre;
 
-// Forward path selection (when Cin % 8 == 0 and Cout % 16 == 0): 0 = warp-level implicit GEMM,
-// 1 = tcgen05 implicit GEMM, 2 (default) = tcgen05 for narrow layers (Cin <= 16 or Cout == 16),
-// where it is faster on B200, and the warp-level kernel for the wider ones, where its 8 warps keep
-// more gathers in flight than the tcgen05 kernel, whose loads for a step wait for the MMAs two
-// steps back (measured per shape, 16^3 to 128^3).
-static std::atomic<int> g_conv_tcgen05{2};
+// Forward path selection: 3 (default) = the tcgen05 halo-tile kernel (conv3d_tc.cu) wherever its
+// shape rules hold (Cin % 16 == 0, Cout % 16 == 0, W % 8 == 0, H % 16 == 0), else mode 2;
+// 0 = warp-level implicit GEMM, 1 = tcgen05 implicit GEMM with per-step gathers, 2 = that
+// tcgen05 kernel for narrow layers (Cin <= 16 or Cout == 16) and the warp-level one for wider ones.
+static std::atomic<int> g_conv_tcgen05{3};
+
+// Per-device status word of the tensor-core convolution kernels (bit 0: a bounded wait expired
+// and that tile was left unwritten), allocated on first use; read by tigre_conv3d_status.
+namespace {
+constexpr int kMaxConvDevices = 64;
+std::mutex g_conv_status_mu;
+int* g_conv_status[kMaxConvDevices] = {};
+
+int* conv_status_word() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxConvDevices) return nullptr;
+    std::lock_guard<std::mutex> lk(g_conv_status_mu);
+    if (!g_conv_status[dev]) {
+        int* p = nullptr;
+        if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) return nullptr;
+        if (cudaMemset(p, 0, sizeof(int)) != cudaSuccess) { cudaFree(p); return nullptr; }
+        g_conv_status[dev] = p;
+    }
+    return g_conv_status[dev];
+}
+}  // namespace
 
 extern "C" {
 
-int tigre_conv3d_set_tcgen05(int mode) { return g_conv_tcgen05.exchange(mode < 0 || mode > 2 ? 2 : mode); }
+int tigre_conv3d_set_tcgen05(int mode) { return g_conv_tcgen05.exchange(mode < 0 || mode > 3 ? 3 : mode); }
+
+int tigre_conv3d_status(int reset) {
+    int* w = conv_status_word();
+    if (!w) return -1;
+    int v = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess) return -1;
+    if (cudaMemcpy(&v, w, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    if (reset && cudaMemset(w, 0, sizeof(int)) != cudaSuccess) return -1;
+    return v;
+}
 
 long long tigre_conv3d_col_elems(long D, long H, long W, long C) { return 27LL * D * H * W * C; }
 
@@ -509,7 +553,14 @@ int tigre_conv3d_fwd(const void* d_x, const void* d_w, const float* d_bias, void
     const long M = D * H * W, K = 27 * Cin;
     if (M * K >= (1L << 31) * 4L || M >= (1L << 31) / 64 * 64) return fail(TIGRE_ERR_BAD_ASSERT, "conv3d too large");
     cudaStream_t st = (cudaStream_t)stream;
-    const int tc_mode = g_conv_tcgen05.load();
+    int tc_mode = g_conv_tcgen05.load();
+    int* status = conv_status_word();
+    if (tc_mode == 3 && ((uintptr_t)d_x & 15) == 0 && ((uintptr_t)d_col & 15) == 0 &&
+        27L * Cin * Cout <= tigre_conv3d_col_elems(D, H, W, Cin) && conv_tc_halo_supported(D, H, W, Cin, Cout))
+        return launch_conv_tc_halo((const __nv_bfloat16*)d_x, (const __nv_bfloat16*)d_w, d_bias,
+                                   (__nv_bfloat16*)d_y_bf16, d_y_f32, D, H, W, Cin, Cout, relu, 0,
+                                   (__nv_bfloat16*)d_col, status, st);
+    if (tc_mode == 3) tc_mode = 2;
     const bool tc_wanted = tc_mode == 1 || (tc_mode == 2 && (Cin <= 16 || Cout == 16));
     if (tc_wanted && Cin % 8 == 0 && Cout % 16 == 0 && ((uintptr_t)d_x & 15) == 0 && ((uintptr_t)d_w & 15) == 0) {
         // tensor-core (tcgen05) implicit GEMM: N tile = the largest of 128 / 64 / 48 / 32 / 16 dividing Cout
@@ -517,11 +568,11 @@ int tigre_conv3d_fwd(const void* d_x, const void* d_w, const float* d_bias, void
         const __nv_bfloat16* wb = (const __nv_bfloat16*)d_w;
         __nv_bfloat16* yb = (__nv_bfloat16*)d_y_bf16;
         const int iD = (int)D, iH = (int)H, iW = (int)W, ci = (int)Cin, co = (int)Cout;
-        if (Cout % 128 == 0) return launch_conv_tc<128>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, nullptr, st);
-        if (Cout % 64 == 0) return launch_conv_tc<64>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, nullptr, st);
-        if (Cout % 48 == 0) return launch_conv_tc<48>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, nullptr, st);
-        if (Cout % 32 == 0) return launch_conv_tc<32>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, nullptr, st);
-        return launch_conv_tc<16>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, nullptr, st);
+        if (Cout % 128 == 0) return launch_conv_tc<128>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, status, st);
+        if (Cout % 64 == 0) return launch_conv_tc<64>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, status, st);
+        if (Cout % 48 == 0) return launch_conv_tc<48>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, status, st);
+        if (Cout % 32 == 0) return launch_conv_tc<32>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, status, st);
+        return launch_conv_tc<16>(xb, wb, d_bias, yb, d_y_f32, iD, iH, iW, ci, co, relu, status, st);
     }
     if (Cin % 8 == 0 && ((uintptr_t)d_x & 15) == 0 && ((uintptr_t)d_w & 15) == 0) {
         // implicit GEMM: 16-byte channel chunks need Cin % 8 == 0 and 16-byte aligned bases
@@ -560,6 +611,13 @@ int tigre_conv3d_bwd_data(const void* d_dy, const void* d_w, float* d_dx, long D
         return fail(TIGRE_ERR_BAD_ASSERT, "bad conv3d arguments");
     const long M = D * H * W, K = 27 * Cin;
     cudaStream_t st = (cudaStream_t)stream;
+    if (g_conv_tcgen05.load() == 3 && ((uintptr_t)d_dy & 15) == 0 && ((uintptr_t)d_dcol & 15) == 0 &&
+        conv_tc_halo_supported(D, H, W, Cout, Cin)) {
+        // the data gradient is the convolution of dy with the tap-flipped, channel-transposed
+        // weights: the halo kernel, FP32 output, no im2col (d_dcol holds the arranged weights)
+        return launch_conv_tc_halo((const __nv_bfloat16*)d_dy, (const __nv_bfloat16*)d_w, nullptr, nullptr, d_dx, D,
+                                   H, W, Cin, Cout, 0, 1, (__nv_bfloat16*)d_dcol, conv_status_word(), st);
+    }
     dim3 grid((unsigned)((M + kBM - 1) / kBM), (unsigned)((K + kBN - 1) / kBN), 1);
     // dcol (M x K) = dy (M x Cout, row-major) . w (Cout x K, row-major)
     gemm_kernel<true, false><<<grid, kThreads, 0, st>>>((const __nv_bfloat16*)d_dy, (int)Cout,
@@ -581,14 +639,27 @@ int tigre_conv3d_bwd_weight(const void* d_x, const void* d_dy, float* d_dw, long
     im2col_kernel<<<grid_for_conv(M * K), 256, 0, st>>>((const __nv_bfloat16*)d_x, (__nv_bfloat16*)d_col, (int)D,
                                                         (int)H, (int)W, (int)Cin);
     TIGRE_LAUNCHED();
-    // the reduction runs over the M voxels: split it over blocks, FP32 atomics into dw
-    const int chunk = 4096;
-    dim3 grid((unsigned)((Cout + kBM - 1) / kBM), (unsigned)((K + kBN - 1) / kBN), (unsigned)((M + chunk - 1) / chunk));
-    // op(A) = dy^T (Cout x M): stored M x Cout row-major -> element (i=co, k=v) at dy[v * Cout + co]
+    // The reduction runs over the M voxels.  It is split over blocks, each writing its partial
+    // dw to its own slice of a stream-ordered workspace, and the slices are then summed in a
+    // fixed order: the result does not depend on the blocks' timing (no atomics).
+    const long per = (long)Cout * K;
+    long splits = std::max(1L, std::min<long>((M + 4095) / 4096, 256));
+    while (splits > 1 && splits * per > (1L << 26)) splits = (splits + 1) / 2;   // <= 256 MB of workspace
+    const long chunk = (M + splits - 1) / splits;
+    splits = (M + chunk - 1) / chunk;
+    float* ws = nullptr;
+    TIGRE_CUDA(cudaMallocAsync(&ws, sizeof(float) * (size_t)(splits * per), st));
+    dim3 grid((unsigned)((Cout + kBM - 1) / kBM), (unsigned)((K + kBN - 1) / kBN), (unsigned)splits);
+    // op(A) = dy^T (Cout x M): stored M x Cout row-major -> element (i=co, k=v) at dy[v * Cout + co];
+    // block z writes rows [0, Cout) x [0, K) of slice z (gemm_kernel's split index offsets K only,
+    // so each slice is addressed through its own C pointer below)
     gemm_kernel<false, false><<<grid, kThreads, 0, st>>>((const __nv_bfloat16*)d_dy, (int)Cout,
-                                                        (const __nv_bfloat16*)d_col, (int)K, d_dw, nullptr, (int)K,
-                                                        (int)Cout, (int)K, (int)M, nullptr, 0, chunk, 1);
+                                                        (const __nv_bfloat16*)d_col, (int)K, ws, nullptr, (int)K,
+                                                        (int)Cout, (int)K, (int)M, nullptr, 0, (int)chunk, 2);
     TIGRE_LAUNCHED();
+    reduce_slices_kernel<<<grid_for_conv(per), 256, 0, st>>>(ws, d_dw, per, splits);
+    TIGRE_LAUNCHED();
+    TIGRE_CUDA(cudaFreeAsync(ws, st));
     return TIGRE_SUCCESS;
 }
 

@@ -171,6 +171,10 @@ int launch_interp(TigrePlan* p, const void* vol_x, const void* vol_y, const void
                   void* proj, int pdt, int a0, int a1, cudaStream_t st);
 int interp_texture(TigrePlan* p, const float* d_vol, cudaStream_t st, unsigned long long* tex_out);
 int launch_interp_tex(TigrePlan* p, unsigned long long tex, void* proj, int pdt, int a0, int a1, cudaStream_t st);
+bool conv_tc_halo_supported(long D, long H, long W, long Cin, long Cout);
+int launch_conv_tc_halo(const __nv_bfloat16* x, const __nv_bfloat16* w, const float* bias, __nv_bfloat16* yb,
+                        float* yf, long D, long H, long W, long Cin, long Cout, int relu, int flip,
+                        __nv_bfloat16* wk_scratch, int* status, cudaStream_t st);
 int launch_backproject(TigrePlan* p, const void* proj_pad, int pdt, void* vol, int vdt, int matched, int a0, int a1,
                        int accumulate, cudaStream_t st);
 
