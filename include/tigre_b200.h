@@ -316,6 +316,23 @@ int tigre_conv3d_bwd_data(const void* d_dy, const void* d_w, float* d_dx, long D
 int tigre_conv3d_bwd_weight(const void* d_x, const void* d_dy, float* d_dw, long D, long H, long W, long Cin,
                             long Cout, void* d_col, void* stream);
 
+/* Fused steps of the warm-start U-Net's inference pass (no reference counterpart), BF16
+ * channels-last activations with FP32 arithmetic; buffers 16-byte aligned.
+ * pool2: y (D/2, H/2, W/2, C) = 2x2x2 mean of x (D, H, W, C); even sizes, C % 8 == 0.
+ * up_concat: out (D, H, W, Ca + Cb) = [nearest 2x upsampling of low (D/2, H/2, W/2, Ca), skip].
+ * conv_in: the first 3x3x3 convolution, one input channel: y (D, H, W, Cout) BF16 from the FP32
+ *   volume rounded to BF16, weights w[Cout][27] BF16, bias FP32 (may be NULL), ReLU if relu;
+ *   Cout 8, 16 or 32.
+ * conv_out: the last 3x3x3 convolution, one output channel: out = vol + bf16(conv(x) + b) (FP32),
+ *   weights w[27 Cin] BF16; Cin 8, 16 or 32. */
+int tigre_unet_pool2(const void* d_x, void* d_y, long D, long H, long W, long C, void* stream);
+int tigre_unet_up_concat(const void* d_low, long Ca, const void* d_skip, long Cb, void* d_out, long D, long H, long W,
+                         void* stream);
+int tigre_unet_conv_in(const float* d_vol, const void* d_w, const float* d_b, void* d_y, long D, long H, long W,
+                       long Cout, int relu, void* stream);
+int tigre_unet_conv_out(const void* d_x, long Cin, const void* d_w, float b, const float* d_vol, float* d_out, long D,
+                        long H, long W, void* stream);
+
 /* FP64 reductions and fused CGLS updates (device scalars, no host round trip). */
 int tigre_sumsq(const void* d_x, int dtype, long n, double* d_out, void* stream);          /* *d_out += sum x^2 */
 int tigre_dot(const float* d_x, const float* d_y, long n, double* d_out, void* stream);    /* *d_out += sum x*y */

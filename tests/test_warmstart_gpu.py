@@ -152,3 +152,57 @@ def test_warmstart_end_to_end_small():
         assert row["plain_zero"]["reached"] and row["warm"]["reached"]
     assert np.isfinite(ev["warm_over_plain_zero"])
     del torch
+
+
+def test_unet_glue_kernels_match_torch():
+    """pool2 / up_concat / conv_in / conv_out of the fused inference pass against the same
+    operations in PyTorch (FP32 reference on the same BF16 values)."""
+    import torch
+    import torch.nn.functional as F
+    from tigre_b200 import _native as N
+    L = N.lib()
+    p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    g = torch.Generator("cuda").manual_seed(7)
+    x = torch.randn((8, 12, 16, 24), device="cuda", generator=g).to(torch.bfloat16)
+    y = torch.empty((4, 6, 8, 24), dtype=torch.bfloat16, device="cuda")
+    N.check(L.tigre_unet_pool2(p(x), p(y), 8, 12, 16, 24, None), "pool2")
+    ref = x.float().view(4, 2, 6, 2, 8, 2, 24).mean(dim=(1, 3, 5))
+    assert float((y.float() - ref).abs().max()) <= float(ref.abs().max()) * 2 ** -7
+    skip = torch.randn((8, 12, 16, 16), device="cuda", generator=g).to(torch.bfloat16)
+    cat = torch.empty((8, 12, 16, 40), dtype=torch.bfloat16, device="cuda")
+    N.check(L.tigre_unet_up_concat(p(y), 24, p(skip), 16, p(cat), 8, 12, 16, None), "up_concat")
+    up = y.repeat_interleave(2, 0).repeat_interleave(2, 1).repeat_interleave(2, 2)
+    assert torch.equal(cat, torch.cat([up, skip], dim=-1))
+    vol = torch.randn((8, 12, 16), device="cuda", generator=g)
+    w = (torch.randn((16, 27), device="cuda", generator=g) / 5).to(torch.bfloat16)
+    b = torch.randn(16, device="cuda", generator=g)
+    h = torch.empty((8, 12, 16, 16), dtype=torch.bfloat16, device="cuda")
+    N.check(L.tigre_unet_conv_in(p(vol), p(w), p(b), p(h), 8, 12, 16, 16, 1, None), "conv_in")
+    xr = vol.to(torch.bfloat16).float()[None, None]
+    ref = F.relu(F.conv3d(xr, w.float().view(16, 1, 3, 3, 3), b, padding=1))[0].permute(1, 2, 3, 0)
+    assert float((h.float() - ref).abs().max()) <= float(ref.abs().max()) * 2 ** -7
+    wo = (torch.randn((1, 27 * 16), device="cuda", generator=g) / 20).to(torch.bfloat16)
+    out = torch.empty_like(vol)
+    N.check(L.tigre_unet_conv_out(p(h), 16, p(wo), 0.25, p(vol), p(out), 8, 12, 16, None), "conv_out")
+    wr = wo.float().view(1, 27, 16).permute(0, 2, 1).reshape(1, 16, 3, 3, 3)
+    conv = F.conv3d(h.float().permute(3, 0, 1, 2)[None], wr, torch.tensor([0.25], device="cuda"), padding=1)[0, 0]
+    ref = vol + conv.to(torch.bfloat16).float()
+    assert float((out - ref).abs().max()) <= float(conv.abs().max()) * 2 ** -7
+
+
+def test_unet_fused_inference_matches_autograd_forward():
+    """UNet3D.infer (fused kernels) against the autograd forward pass on the same weights."""
+    import torch
+    from tigre_b200 import warmstart as WS
+    model = WS.unet(seed=3)
+    vol = torch.rand((64, 64, 64), device="cuda", generator=torch.Generator("cuda").manual_seed(4))
+    with torch.no_grad():
+        fused = model(vol)
+    with torch.enable_grad():
+        plain = model(vol).detach()
+    d = fused - vol
+    r = plain - vol
+    mx = float((d - r).abs().max() / r.abs().max())
+    l2 = float(torch.linalg.vector_norm(d - r) / torch.linalg.vector_norm(r))
+    print("fused vs autograd U-Net output: max %.2e, L2 %.2e" % (mx, l2))
+    assert mx <= 3e-2 and l2 <= 1e-2, (mx, l2)

@@ -118,6 +118,13 @@ _SIGS = {
     "tigre_conv3d_col_elems": (C.c_longlong, [C.c_long, C.c_long, C.c_long, C.c_long]),
     "tigre_conv3d_set_tcgen05": (C.c_int, [C.c_int]),
     "tigre_conv3d_status": (C.c_int, [C.c_int]),
+    "tigre_unet_pool2": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long, C.c_long, C.c_long, C.c_long, C.c_void_p]),
+    "tigre_unet_up_concat": (C.c_int, [C.c_void_p, C.c_long, C.c_void_p, C.c_long, C.c_void_p, C.c_long, C.c_long,
+                                       C.c_long, C.c_void_p]),
+    "tigre_unet_conv_in": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_long, C.c_long,
+                                     C.c_long, C.c_int, C.c_void_p]),
+    "tigre_unet_conv_out": (C.c_int, [C.c_void_p, C.c_long, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_long,
+                                      C.c_long, C.c_long, C.c_void_p]),
     "tigre_conv3d_fwd": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_long,
                                    C.c_long, C.c_long, C.c_long, C.c_int, C.c_void_p, C.c_void_p]),
     "tigre_conv3d_bwd_data": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_long, C.c_long, C.c_long,

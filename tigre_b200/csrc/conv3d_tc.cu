@@ -161,14 +161,18 @@ __global__ void __launch_bounds__(128, 1) conv_tc_halo_kernel(const __grid_const
                              su32(&empty_bar[s]))
                          : "memory");
             ++issued_mma;
-            // refill the stage of chunk c - 1 with chunk c - 1 + stages once its MMAs have read it
-            const int nxt = c - 1 + p.stages;
-            if (c >= 1 && nxt < p.nchunks) {
-                const int sp = (c - 1) % p.stages;
+            // keep the loads ahead: up to chunk c + stages - 1 (with one stage, chunk c + 1), each
+            // into the stage of chunk L - stages once the MMAs of that chunk have read it -- with
+            // two or more stages those are the MMAs of chunk c - 1, queued before the ones just
+            // issued, so the copy overlaps the MMAs of chunk c
+            const int target = c + max(p.stages - 1, 1);
+            while (ok && issued_loads <= target && issued_loads < p.nchunks) {
+                const int sp = (issued_loads - p.stages) % p.stages;
                 if (!bar_wait(su32(&empty_bar[sp]), (empty_ph >> sp) & 1u)) { ok = false; break; }
                 empty_ph ^= 1u << sp;
-                load(nxt);
+                load(issued_loads);
             }
+            if (!ok) break;
         }
         if (ok) {
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -282,18 +286,23 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
 
 }  // namespace
 
-// z-slices per tile and pipeline stages for an N-channel output, within 200 KB of shared memory
-static void conv_tc_shape(int N, int D, int* zt, int* stages, uint32_t* tile_bytes, uint32_t* w_bytes) {
+// z-slices per tile and pipeline stages for an N-channel output with nchunks input chunks.
+// Several CTAs per SM overlap one CTA's loads and epilogue with another's MMAs, so a
+// configuration that fits two or more CTAs per SM (<= 112 KB) is preferred, with as many
+// stages (<= nchunks, <= 3) as fit; else one CTA per SM within 200 KB.
+static void conv_tc_shape(int N, int D, int nchunks, int* zt, int* stages, uint32_t* tile_bytes, uint32_t* w_bytes) {
     const int cand[3] = {4, 2, 1};
-    for (int i = 0; i < 3; ++i) {
-        const int z = cand[i];
-        if (D % z) continue;
-        const uint32_t tb = (uint32_t)(kHx * kHy * (z + 2) * kCC * 2), wb = (uint32_t)(27 * kCC * N * 2);
-        const uint32_t stb = (tb + wb + 1023u) & ~1023u;
-        if ((size_t)z * N > 512) continue;
-        for (int s = 3; s >= 1; --s) {
-            if (1024 + (size_t)s * stb <= 200 * 1024) {
-                if (s >= 2 || i == 2) {
+    *zt = 0;
+    for (int budget : {112 * 1024, 200 * 1024}) {
+        for (int i = 0; i < 3; ++i) {
+            const int z = cand[i];
+            if (D % z || (size_t)z * N > 512) continue;
+            const uint32_t tb = (uint32_t)(kHx * kHy * (z + 2) * kCC * 2), wb = (uint32_t)(27 * kCC * N * 2);
+            const uint32_t stb = (tb + wb + 1023u) & ~1023u;
+            for (int s = std::min(3, nchunks); s >= 1; --s) {
+                if (1024 + (size_t)s * stb > (size_t)budget) continue;
+                // fewer than two stages only when there is a single chunk, or as the last resort
+                if (s >= std::min(2, nchunks) || (budget > 112 * 1024 && i == 2)) {
                     *zt = z; *stages = s; *tile_bytes = tb; *w_bytes = wb;
                     return;
                 }
@@ -301,14 +310,13 @@ static void conv_tc_shape(int N, int D, int* zt, int* stages, uint32_t* tile_byt
             }
         }
     }
-    *zt = 0;
 }
 
 bool conv_tc_halo_supported(long D, long H, long W, long Cin, long Cout) {
     if (Cin % kCC || Cout % 16 || Cout < 16 || Cout > 256 || W % kTx || H % kTy) return false;
     int zt, st;
     uint32_t tb, wb;
-    conv_tc_shape((int)Cout, (int)D, &zt, &st, &tb, &wb);
+    conv_tc_shape((int)Cout, (int)D, (int)(Cin / kCC), &zt, &st, &tb, &wb);
     return zt > 0 && encode_tiled() != nullptr && D * H * W < (1L << 31);
 }
 
@@ -325,7 +333,7 @@ int launch_conv_tc_halo(const __nv_bfloat16* x, const __nv_bfloat16* w, const fl
     if (!conv_tc_halo_supported(D, H, W, K, N)) return fail(TIGRE_ERR_BAD_ASSERT, "conv shape not supported by the halo kernel");
     int zt, stages;
     uint32_t tb, wb;
-    conv_tc_shape((int)N, (int)D, &zt, &stages, &tb, &wb);
+    conv_tc_shape((int)N, (int)D, (int)(K / kCC), &zt, &stages, &tb, &wb);
     const long total = 27L * K * N;
     arrange_weights_kernel<<<(int)std::min<long>((total + 255) / 256, 148L * 16), 256, 0, st>>>(w, wk_scratch, (int)Cin,
                                                                                                 (int)Cout, flip);
