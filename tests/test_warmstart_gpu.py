@@ -190,19 +190,50 @@ def test_unet_glue_kernels_match_torch():
     assert float((out - ref).abs().max()) <= float(conv.abs().max()) * 2 ** -7
 
 
+def _unet_fp32_reference(model, vol):
+    """The same network in FP32 (torch conv3d on BF16-rounded weights, FP32 activations)."""
+    import torch
+    import torch.nn.functional as F
+
+    def conv(x, layer):
+        cout, k = layer.w.shape
+        cin = k // 27
+        w = layer.w.detach().to(torch.bfloat16).float().view(cout, 27, cin).permute(0, 2, 1).reshape(cout, cin, 3, 3, 3)
+        y = F.conv3d(x, w, layer.b.detach(), padding=1)
+        return F.relu(y) if layer.relu else y
+
+    x = vol.to(torch.bfloat16).float()[None, None]
+    skips = []
+    for i, (c1, c2) in enumerate(model.enc):
+        x = conv(conv(x, c1), c2)
+        if i < len(model.enc) - 1:
+            skips.append(x)
+            x = F.avg_pool3d(x, 2)
+    for (c1, c2), s in zip(model.dec, reversed(skips)):
+        x = torch.cat([F.interpolate(x, scale_factor=2, mode="nearest"), s], dim=1)
+        x = conv(conv(x, c1), c2)
+    return vol + conv(x, model.head)[0, 0]
+
+
 def test_unet_fused_inference_matches_autograd_forward():
-    """UNet3D.infer (fused kernels) against the autograd forward pass on the same weights."""
+    """UNet3D.infer (fused kernels) and the autograd forward pass on the same weights, both
+    against the network in FP32: BF16 activations put each within a few 1e-2 (L2) of it, and
+    the fused pass is no further from it than the autograd one (within 25 %)."""
     import torch
     from tigre_b200 import warmstart as WS
     model = WS.unet(seed=3)
     vol = torch.rand((64, 64, 64), device="cuda", generator=torch.Generator("cuda").manual_seed(4))
     with torch.no_grad():
         fused = model(vol)
+        ref = _unet_fp32_reference(model, vol)
     with torch.enable_grad():
         plain = model(vol).detach()
-    d = fused - vol
-    r = plain - vol
-    mx = float((d - r).abs().max() / r.abs().max())
-    l2 = float(torch.linalg.vector_norm(d - r) / torch.linalg.vector_norm(r))
-    print("fused vs autograd U-Net output: max %.2e, L2 %.2e" % (mx, l2))
-    assert mx <= 3e-2 and l2 <= 1e-2, (mx, l2)
+    r = ref - vol
+
+    def err(a):
+        d = a - vol - r
+        return float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(r))
+
+    e_f, e_p = err(fused), err(plain)
+    print("U-Net vs FP32 network (L2): fused %.3e, autograd %.3e" % (e_f, e_p))
+    assert e_f <= 5e-2 and e_p <= 5e-2 and e_f <= 1.25 * e_p + 1e-3, (e_f, e_p)
