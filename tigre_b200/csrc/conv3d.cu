@@ -551,7 +551,6 @@ int tigre_conv3d_fwd(const void* d_x, const void* d_w, const float* d_bias, void
     if (!d_x || !d_w || !d_col || (!d_y_bf16 && !d_y_f32) || D <= 0 || H <= 0 || W <= 0 || Cin <= 0 || Cout <= 0)
         return fail(TIGRE_ERR_BAD_ASSERT, "bad conv3d arguments");
     const long M = D * H * W, K = 27 * Cin;
-    if (M * K >= (1L << 31) * 4L || M >= (1L << 31) / 64 * 64) return fail(TIGRE_ERR_BAD_ASSERT, "conv3d too large");
     cudaStream_t st = (cudaStream_t)stream;
     int tc_mode = g_conv_tcgen05.load();
     int* status = conv_status_word();
@@ -561,6 +560,8 @@ int tigre_conv3d_fwd(const void* d_x, const void* d_w, const float* d_bias, void
                                    (__nv_bfloat16*)d_y_bf16, d_y_f32, D, H, W, Cin, Cout, relu, 0,
                                    (__nv_bfloat16*)d_col, status, st);
     if (tc_mode == 3) tc_mode = 2;
+    // the other paths index the im2col matrix (M x 27 Cin) with 32-bit row counts
+    if (M * K >= (1L << 31) * 4L || M >= (1L << 31) / 64 * 64) return fail(TIGRE_ERR_BAD_ASSERT, "conv3d too large");
     const bool tc_wanted = tc_mode == 1 || (tc_mode == 2 && (Cin <= 16 || Cout == 16));
     if (tc_wanted && Cin % 8 == 0 && Cout % 16 == 0 && ((uintptr_t)d_x & 15) == 0 && ((uintptr_t)d_w & 15) == 0) {
         // tensor-core (tcgen05) implicit GEMM: N tile = the largest of 128 / 64 / 48 / 32 / 16 dividing Cout
