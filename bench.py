@@ -268,11 +268,19 @@ def measure_cgls():
     from tigre_b200.algorithms.krylov import cgls_device
     from tigre_b200.algorithms.single_pass import fdk_device
     from tigre_b200.utilities.phantom import random_ellipsoids
+    from tigre_b200 import warmstart as WS
     geo, ang = c5_geometry(), c5_angles()
     img = random_ellipsoids((C5_VOX,) * 3, seed=0, device="cuda")
     plan = N.get_plan(N.checked_geometry(geo, ang), img.device.index)
     clean = P.ax(img, plan, "Siddon")
     out = {"workload": C5_WORKLOAD}
+    model = WS.pretrained_c5()
+    if model is not None:
+        out["warm_start"] = ("3-D U-Net (4 levels, 16 base channels, BF16, FP32 accumulation) trained by this "
+                             "library's kernels on 96 seeded 256^3 phantoms of this configuration (I0 = 5e4), "
+                             "weights in tigre_b200/data; its inference is timed with FDK")
+        with torch.no_grad():
+            model(torch.zeros((C5_VOX,) * 3, device="cuda"))     # warm-up of the inference kernels
 
     def run(prob, x0, target):
         torch.cuda.synchronize()
@@ -308,6 +316,20 @@ def measure_cgls():
         fr["fdk_s"] = round(t_fdk, 4)
         fr["s"] = round(fr["s"] + t_fdk, 4)
         row["fdk"] = fr
+        if model is not None:
+            # learned warm start: FDK, U-Net inference, CGLS from its output (all timed)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            with torch.no_grad():
+                x0 = (model(fdk_device(prob) * WS.SCALE) / WS.SCALE).contiguous()
+            torch.cuda.synchronize()
+            t_inf = time.perf_counter() - t
+            wr = run(prob, x0, target)
+            wr["fdk_and_inference_s"] = round(t_inf, 4)
+            wr["s"] = round(wr["s"] + t_inf, 4)
+            row["warm"] = wr
+            row["warm_over_zero"] = round(wr["s"] / row["zero"]["s"], 3)
+            row["warm_over_fdk"] = round(wr["s"] / fr["s"], 3)
         out[variant] = row
     return out
 
