@@ -191,6 +191,7 @@ __global__ void __launch_bounds__(TXY* TXY, 2) bp_tma_kernel(const __grid_consta
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) unsigned long long bars[2];
     __shared__ int info[2][4];
+    __shared__ volatile int fail_flag;   // set by any thread whose wait expired, read after a barrier
     // TMA destinations: 128-byte aligned, each buffer rounded up to 128 bytes
     const uint32_t base_off = (128u - (smem_u32(smem_raw) & 127u)) & 127u;
     const size_t buf_bytes = ((size_t)p.BU * p.BV * sizeof(TP) + 127) / 128 * 128;
@@ -208,6 +209,7 @@ __global__ void __launch_bounds__(TXY* TXY, 2) bp_tma_kernel(const __grid_consta
     const bool active = x < p.nX && y < p.nY;
     const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
     if (tid == 0) {
+        fail_flag = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -383,7 +385,9 @@ __global__ void __launch_bounds__(TXY* TXY, 2) bp_tma_kernel(const __grid_consta
         }
         // everyone is done with buffer s; a wait that expired in any thread stops the whole
         // block before buffer s is refilled or its barrier re-armed
-        if (__syncthreads_or(!ok)) {
+        if (!ok) fail_flag = 1;
+        __syncthreads();
+        if (fail_flag) {
             failed_at = la;
             break;
         }
