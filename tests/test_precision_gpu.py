@@ -152,3 +152,35 @@ def test_ossart_per_iteration_vs_fp64_oracle(order):
         print("%s %s %s per-iteration rel L2 vs FP64 oracle: %s" % (order, dtype, rounding,
                                                                      " ".join("%.2e" % e for e in errs)))
         assert len(errs) == niter and max(errs) <= bound, (dtype, rounding, errs)
+
+
+def test_precision_configuration_scaled_per_iteration_vs_fp64_oracle():
+    """The precision configuration (512^3 @ 0.5 mm, 1024 x 768 @ 0.4 mm, 720 views, 20 OS-SART
+    iterations of 20 subsets) scaled by 1/4 per axis so that the FP64 oracle's whole trajectory
+    is affordable on the host: 128^3 @ 2 mm (256 mm), 256 x 192 @ 1.6 mm, 180 views, blocksize 9
+    (20 subsets), 20 iterations.  Per iteration, the relative L2 error of the FP32 path and of
+    BF16 storage (nearest and stochastic rounding) against the FP64 oracle OS-SART."""
+    import torch
+    import tigre_b200 as tigre
+    from tigre_b200.utilities.geometry import cone_geometry
+    from tigre_b200.utilities.order_subsets import order_subsets
+    geo = cone_geometry((128, 128, 128), (256.0, 256.0, 256.0), (192, 256), (1.6, 1.6), DSO=1000.0, DSD=1536.0)
+    ang = np.linspace(0, 2 * np.pi, 180, endpoint=False).astype(np.float32)
+    img = G.phantom((128, 128, 128), seed=0)
+    proj = O.ax(img, geo, ang, "Siddon")
+    ang3 = np.zeros((180, 3), dtype=np.float32)
+    ang3[:, 0] = ang
+    _, index = order_subsets(ang3, 9, None)
+    niter = 20
+    ref = []
+    O.ossart(proj, geo, ang, niter, index, callback=lambda it, x: ref.append(x.copy()))
+    bounds = {("float32", "nearest"): 1e-4, ("bfloat16", "nearest"): 3e-2, ("bfloat16", "stochastic"): 3e-2}
+    for (dtype, rounding), bound in bounds.items():
+        got = []
+        st = None if dtype == "float32" else getattr(torch, dtype)
+        tigre.algorithms.ossart(proj, geo, ang, niter, blocksize=9, storage=st, rounding=rounding, seed=5,
+                                callback=lambda it, x: got.append(x.double().cpu().numpy()))
+        errs = [np.linalg.norm(g - r) / np.linalg.norm(r) for g, r in zip(got, ref)]
+        print("scaled precision configuration, %s %s, per-iteration rel L2 vs FP64 oracle: %s" % (
+            dtype, rounding, " ".join("%.2e" % e for e in errs)))
+        assert len(errs) == niter and max(errs) <= bound, (dtype, rounding, errs)
