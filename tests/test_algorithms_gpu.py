@@ -390,3 +390,20 @@ def test_fista_matches_oracle_and_ista_runs():
     assert mx <= 1e-4 and l2 <= 1e-5, (mx, l2)
     x, l2s = tigre.algorithms.ista(proj, geo, ang, 2, hyper=hyper, computel2=True)
     assert np.isfinite(x).all() and l2s.shape == (1, 2)
+
+
+def test_quameasopts_reporting():
+    """Quameasopts (iterative_recon_alg.py:205-209, :362-364): per iteration, the quality
+    measures between the new and the previous iterate; with computel2 the residual row comes
+    first (geterrors, :406-410)."""
+    import tigre_b200 as tigre
+    from tigre_b200.utilities.Measure_Quality import Measure_Quality
+    geo, ang, img = _case(views=20)
+    proj = O.ax(img, geo, ang, "Siddon")
+    x, err = tigre.algorithms.ossart(proj, geo, ang, 3, blocksize=5, Quameasopts=["RMSE", "CC"], computel2=True)
+    assert err.shape == (3, 3) and np.all(np.diff(err[0]) < 0)
+    x1 = tigre.algorithms.ossart(proj, geo, ang, 1, blocksize=5)
+    x2 = tigre.algorithms.ossart(proj, geo, ang, 2, blocksize=5)
+    np.testing.assert_allclose(err[1:, 1], Measure_Quality(x2, x1, ["RMSE", "CC"]), rtol=1e-4)
+    xc, q = tigre.algorithms.cgls(proj, geo, ang, 4, Quameasopts="RMSE")
+    assert q.shape == (1, 4) and np.all(q > 0)

@@ -192,3 +192,16 @@ def test_parker_weights_follow_u_on_a_wide_detector():
     # every ray is weighted once over the short scan: opposite rays sum to one in the interior
     from tigre_b200.utilities import filtering as F
     np.testing.assert_allclose(F.parker_weights(geo, ang), w, atol=2e-7)
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_measure_quality_matches_reference(seed):
+    """tigre_b200.utilities.Measure_Quality against the reference's own outputs."""
+    from tests.golden.make_quality_golden import OPTS, pair
+    from tigre_b200.utilities.Measure_Quality import Measure_Quality
+    ref = np.load(os.path.join(HERE, "golden", "ref_quality.npz"))["seed%d" % seed]
+    a, b = pair(seed)
+    got = Measure_Quality(a, b, OPTS)
+    np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-12)
+    for i, q in enumerate(OPTS):
+        np.testing.assert_allclose(Measure_Quality(a, b, q), ref[i], rtol=1e-6, atol=1e-12)

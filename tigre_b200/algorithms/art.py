@@ -27,6 +27,7 @@ import numpy as np
 from .. import _native as N
 from .. import projectors as P
 from ..utilities.order_subsets import order_subsets
+from ..utilities.Measure_Quality import QualityLog
 from ._common import Problem, torch
 
 
@@ -133,16 +134,21 @@ def _run(proj, geo, angles, niter, blocksize, kwargs):
         x = x.to(storage)
     l2 = []
     callback = kwargs.get("callback")
+    quality = QualityLog(kwargs.get("Quameasopts"), niter)
     for it in range(niter):
+        quality.before(x)
         art.sweep(x)
         if kwargs.get("computel2", False):
             l2.append(float(T.linalg.vector_norm((prob.b - P.ax(x, prob.plan, "Siddon", out_dtype=T.float32))
                                                  .double()).item()))
+        quality.after(x, it)
         if callback is not None:
             callback(it, x)
     out = prob.out(x.float() if x.dtype != T.float32 else x)
-    if kwargs.get("computel2", False):
+    if kwargs.get("computel2", False) and not quality.active:
         return out, np.asarray(l2, dtype=np.float32).reshape(1, -1)
+    if quality.active:
+        return out, quality.errors(l2 if kwargs.get("computel2", False) else None)
     return out
 
 

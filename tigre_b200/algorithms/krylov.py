@@ -27,6 +27,7 @@ import time
 import numpy as np
 
 from .. import projectors as P
+from ..utilities.Measure_Quality import QualityLog
 from ._common import Problem, torch
 
 
@@ -124,9 +125,20 @@ def cgls(proj, geo, angles, niter, **kwargs):
             raise ValueError("wrong value for initialization")
     elif init is not None:
         x0 = init
+    quality = QualityLog(kwargs.get("Quameasopts"), niter)
+    callback = None
+    if quality.active:
+        quality.before(prob.to_device_vol(x0) if x0 is not None else prob.zeros_vol())
+
+        def callback(it, x, rel):
+            quality.after(x, it)
+            quality.before(x)
     x, l2, _ = cgls_device(prob, niter, x0=x0, tol=kwargs.get("tol"), true_residual=kwargs.get("true_residual", False),
-                           restart=kwargs.get("restart", True), verbose=kwargs.get("verbose", False))
+                           restart=kwargs.get("restart", True), verbose=kwargs.get("verbose", False),
+                           callback=callback)
     out = prob.out(x)
+    if quality.active:
+        return out, quality.errors(l2 if kwargs.get("computel2", False) else None)
     if kwargs.get("computel2", False) or kwargs.get("return_residuals", False):
         return out, l2.reshape(1, -1).astype(np.float32)
     return out
