@@ -179,6 +179,7 @@ extern "C" {
 
 int tigre_ax(TigrePlan* plan, const void* d_vol, int vdt, void* d_proj, int pdt, int projector, int a0, int a1,
              void* stream) {
+    TIGRE_NVTX("tigre_ax");
     if (int rc = check_range(plan, a0, a1)) return rc;
     if (!d_vol || !d_proj) return fail(TIGRE_ERR_BAD_ASSERT, "null device pointer");
     if (!dtype_ok(vdt) || !dtype_ok(pdt)) return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype");
@@ -196,6 +197,7 @@ int tigre_atb(TigrePlan* plan, const void* d_proj, int pdt, void* d_vol, int vdt
 
 int tigre_atb_ex(TigrePlan* plan, const void* d_proj, int pdt, void* d_vol, int vdt, int backprojector, int a0, int a1,
                  int accumulate, void* stream) {
+    TIGRE_NVTX("tigre_atb");
     if (int rc = check_range(plan, a0, a1)) return rc;
     if (!d_vol || !d_proj) return fail(TIGRE_ERR_BAD_ASSERT, "null device pointer");
     if (!dtype_ok(vdt) || !dtype_ok(pdt)) return fail(TIGRE_ERR_BAD_ASSERT, "unsupported dtype");
@@ -502,6 +504,7 @@ int take_status(TigrePlan* plan, cudaStream_t st, int* out) {
 
 int host_project(const float* img, const TigreGeometry* geo, float* const* result, const float* angles, int nangles,
                  const int* ids, int n, int projector, int flags = 0) {
+    TIGRE_NVTX("host projection");
     if (!img || !geo || !result || !angles) return fail(TIGRE_ERR_BAD_ASSERT, "null argument");
     int dev = 0;
     if (int rc = pick_device(ids, n, &dev)) return rc;
@@ -554,6 +557,7 @@ int host_project(const float* img, const TigreGeometry* geo, float* const* resul
 
 int host_backproject(const float* proj, const TigreGeometry* geo, float* result, const float* angles, int nangles,
                      const int* ids, int n, int matched, int flags = 0) {
+    TIGRE_NVTX("host backprojection");
     if (!proj || !geo || !result || !angles) return fail(TIGRE_ERR_BAD_ASSERT, "null argument");
     int dev = 0;
     if (int rc = pick_device(ids, n, &dev)) return rc;
@@ -602,6 +606,7 @@ int host_backproject(const float* proj, const TigreGeometry* geo, float* result,
 
 int host_pocs_tv(const float* img, float* dst, float alpha, const long* image_size, int max_iter, const int* ids,
                  int n) {
+    TIGRE_NVTX("host pocs_tv");
     if (!img || !dst || !image_size) return fail(TIGRE_ERR_BAD_ASSERT, "null argument");
     const long nx = image_size[0], ny = image_size[1], nz = image_size[2];
     if (nx <= 0 || ny <= 0 || nz <= 0) return fail(TIGRE_ERR_BAD_ASSERT, "bad image size");
@@ -622,6 +627,7 @@ int host_pocs_tv(const float* img, float* dst, float alpha, const long* image_si
 
 int host_weighted_tv(int kind, const float* img, const float* prior, float* dst, float alpha, float param,
                      const long* image_size, int max_iter, const int* ids, int n) {
+    TIGRE_NVTX("host weighted tv");
     if (!img || !dst || !image_size || (kind == 1 && !prior)) return fail(TIGRE_ERR_BAD_ASSERT, "null argument");
     const long nx = image_size[0], ny = image_size[1], nz = image_size[2];
     if (nx <= 0 || ny <= 0 || nz <= 0) return fail(TIGRE_ERR_BAD_ASSERT, "bad image size");
@@ -649,6 +655,7 @@ int host_weighted_tv(int kind, const float* img, const float* prior, float* dst,
 
 int host_tvdenoising(const float* src, float* dst, float lambda, const float* spacing, const long* image_size,
                      int max_iter, const int* ids, int n) {
+    TIGRE_NVTX("host tvdenoising");
     if (!src || !dst || !image_size) return fail(TIGRE_ERR_BAD_ASSERT, "null argument");
     const long nx = image_size[0], ny = image_size[1], nz = image_size[2];
     if (nx <= 0 || ny <= 0 || nz <= 0) return fail(TIGRE_ERR_BAD_ASSERT, "bad image size");

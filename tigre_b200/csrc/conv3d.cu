@@ -548,6 +548,7 @@ long long tigre_conv3d_col_elems(long D, long H, long W, long C) { return 27LL *
 
 int tigre_conv3d_fwd(const void* d_x, const void* d_w, const float* d_bias, void* d_y_bf16, float* d_y_f32, long D,
                      long H, long W, long Cin, long Cout, int relu, void* d_col, void* stream) {
+    TIGRE_NVTX("tigre_conv3d_fwd");
     if (!d_x || !d_w || !d_col || (!d_y_bf16 && !d_y_f32) || D <= 0 || H <= 0 || W <= 0 || Cin <= 0 || Cout <= 0)
         return fail(TIGRE_ERR_BAD_ASSERT, "bad conv3d arguments");
     const long M = D * H * W, K = 27 * Cin;
@@ -608,6 +609,7 @@ int tigre_conv3d_fwd(const void* d_x, const void* d_w, const float* d_bias, void
 // dx (FP32, channels-last) from dy (BF16, M x Cout) and w; d_dcol: M * 27*Cin floats of scratch.
 int tigre_conv3d_bwd_data(const void* d_dy, const void* d_w, float* d_dx, long D, long H, long W, long Cin, long Cout,
                           float* d_dcol, void* stream) {
+    TIGRE_NVTX("tigre_conv3d_bwd_data");
     if (!d_dy || !d_w || !d_dx || !d_dcol || D <= 0 || H <= 0 || W <= 0 || Cin <= 0 || Cout <= 0)
         return fail(TIGRE_ERR_BAD_ASSERT, "bad conv3d arguments");
     const long M = D * H * W, K = 27 * Cin;
@@ -633,6 +635,7 @@ int tigre_conv3d_bwd_data(const void* d_dy, const void* d_w, float* d_dx, long D
 // dw (FP32, Cout x 27*Cin) += dy^T . col, with col = im2col(x) recomputed into d_col.
 int tigre_conv3d_bwd_weight(const void* d_x, const void* d_dy, float* d_dw, long D, long H, long W, long Cin,
                             long Cout, void* d_col, void* stream) {
+    TIGRE_NVTX("tigre_conv3d_bwd_weight");
     if (!d_x || !d_dy || !d_dw || !d_col || D <= 0 || H <= 0 || W <= 0 || Cin <= 0 || Cout <= 0)
         return fail(TIGRE_ERR_BAD_ASSERT, "bad conv3d arguments");
     const long M = D * H * W, K = 27 * Cin;

@@ -181,6 +181,7 @@ extern "C" {
 int tigre_sart_update(void* d_x, int dtype, const float* d_bp, const float* d_v, float lambda, int noneg,
                       long long nz, long long nyx, int rounding, unsigned long long seed, unsigned long long step,
                       void* stream) {
+    TIGRE_NVTX("tigre_sart_update");
     if (!dtype_ok(dtype)) return fail(TIGRE_ERR_BAD_ASSERT, "sart_update: unknown storage dtype");
     if (nz < 0 || nyx < 0) return fail(TIGRE_ERR_BAD_ASSERT, "sart_update: negative size");
     if (rounding != TIGRE_ROUND_NEAREST && rounding != TIGRE_ROUND_STOCHASTIC)

@@ -373,6 +373,7 @@ int tigre_tv_value(const void* d_img, int dtype, long nx, long ny, long nz, doub
 // reduction scratch are taken from the stream-ordered allocator.
 int tigre_tv_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha, int max_iter, float* d_work,
                   void* stream) {
+    TIGRE_NVTX("tigre_tv_pocs");
     if (dtype != TIGRE_F32) return fail(TIGRE_ERR_BAD_ASSERT, "TV kernels take float32 volumes");
     if (nx <= 0 || ny <= 0 || nz <= 0 || !d_img || !d_work || max_iter < 0)
         return fail(TIGRE_ERR_BAD_ASSERT, "bad TV arguments");
@@ -428,6 +429,7 @@ extern "C" {
 //   g = grad AwTV(f);  f <- f - alpha g / sqrt(sum g^2 + 1e-7).
 int tigre_tv_aw_pocs(void* d_img, int dtype, long nx, long ny, long nz, float alpha, int max_iter, float delta,
                     float* d_work, void* stream) {
+    TIGRE_NVTX("tigre_tv_aw_pocs");
     if (dtype != TIGRE_F32) return fail(TIGRE_ERR_BAD_ASSERT, "TV kernels take float32 volumes");
     if (nx <= 0 || ny <= 0 || nz <= 0 || !d_img || !d_work || max_iter < 0)
         return fail(TIGRE_ERR_BAD_ASSERT, "bad TV arguments");
@@ -441,6 +443,7 @@ int tigre_tv_aw_pocs(void* d_img, int dtype, long nx, long ny, long nz, float al
 //   g = (1 - ratio) grad TV(f) + ratio grad TV(f - prior);  f <- f - alpha g / sqrt(sum g^2).
 int tigre_tv_piccs(void* d_img, const void* d_prior, int dtype, long nx, long ny, long nz, float alpha, float ratio,
                    int max_iter, float* d_work, void* stream) {
+    TIGRE_NVTX("tigre_tv_piccs");
     if (dtype != TIGRE_F32) return fail(TIGRE_ERR_BAD_ASSERT, "TV kernels take float32 volumes");
     if (nx <= 0 || ny <= 0 || nz <= 0 || !d_img || !d_prior || !d_work || max_iter < 0)
         return fail(TIGRE_ERR_BAD_ASSERT, "bad TV arguments");

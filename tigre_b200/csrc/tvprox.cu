@@ -88,6 +88,7 @@ long long tigre_tv_denoise_work_floats(long nx, long ny, long nz) {
 
 int tigre_tv_denoise(const float* d_src, float* d_dst, long nx, long ny, long nz, float lambda, const float* spacing,
                      int max_iter, float* d_work, void* stream) {
+    TIGRE_NVTX("tigre_tv_denoise");
     if (!d_src || !d_dst || !d_work || nx <= 0 || ny <= 0 || nz <= 0 || max_iter < 0)
         return fail(TIGRE_ERR_BAD_ASSERT, "bad TV denoising arguments");
     if (!(lambda > 0.f)) return fail(TIGRE_ERR_BAD_ASSERT, "TV denoising: lambda must be positive");
