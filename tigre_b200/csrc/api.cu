@@ -375,7 +375,7 @@ std::vector<DeviceState*> g_states;
 // buffers keep the direct path.
 constexpr size_t kStageBytes = (size_t)64 << 20;
 constexpr size_t kStageMin = (size_t)32 << 20;
-constexpr unsigned kStageThreads = 8;
+constexpr unsigned kStageThreads = 16;
 
 // which (bit mask, option TIGRE_OPT_HOST_STAGING, default kStageDefault): 1 uploads of a volume, 2 downloads
 // of a volume, 4 the backprojector's projection-chunk uploads, 8 the backprojector's volume
