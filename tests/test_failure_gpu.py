@@ -3,8 +3,9 @@ device stays usable.
 
 TIGRE_OPT_BP_SKIP_COPY makes the TMA-staged backprojector issue no copy (and no arrival) for
 one view of each launch, so every block's bounded mbarrier wait for that view runs out with
-nothing in flight.  The kernel then stops the block, waits for the copy of the next view
-that was already issued, sets TIGRE_STATUS_WAIT_EXPIRED in the plan status word and exits;
+nothing in flight.  The threads then wait no more, no further copy is issued, thread 0
+waits for the copy of the next view that was already issued, and the block writes nothing,
+sets TIGRE_STATUS_WAIT_EXPIRED in the plan status word and exits;
 the device call returns normally (the status is the report), the host call returns
 TIGRE_ERR_CUDA.  Afterwards the same plan and the host entry points give correct results.
 """
