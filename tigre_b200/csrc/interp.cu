@@ -19,6 +19,7 @@
 //    8-corner gather needs no bounds tests.
 
 #include <climits>
+#include <type_traits>
 #include <cmath>
 
 #include "tigre_internal.h"
@@ -56,10 +57,18 @@ template <> __device__ __forceinline__ float4 ldq<__half>(const void* base, uint
     return make_float4(a.x, a.y, b.x, b.y);
 }
 
-// trilinear value from the quads of rows o and o+1 (fractions along fast, z, other)
+// trilinear value from the quads of rows o and o+1 (fractions along fast, z, other); FP32
+// quads carry the fast-axis differences already (make_quads_kernel), 16-bit ones the corners
+template <typename TV>
 __device__ __forceinline__ float tri(const float4 q0, const float4 q1, float ff, float fz, float fo) {
-    const float a0 = fmaf(ff, q0.y - q0.x, q0.x), a1 = fmaf(ff, q0.w - q0.z, q0.z);
-    const float b0 = fmaf(ff, q1.y - q1.x, q1.x), b1 = fmaf(ff, q1.w - q1.z, q1.z);
+    float a0, a1, b0, b1;
+    if constexpr (std::is_same<TV, float>::value) {
+        a0 = fmaf(ff, q0.y, q0.x), a1 = fmaf(ff, q0.w, q0.z);
+        b0 = fmaf(ff, q1.y, q1.x), b1 = fmaf(ff, q1.w, q1.z);
+    } else {
+        a0 = fmaf(ff, q0.y - q0.x, q0.x), a1 = fmaf(ff, q0.w - q0.z, q0.z);
+        b0 = fmaf(ff, q1.y - q1.x, q1.x), b1 = fmaf(ff, q1.w - q1.z, q1.z);
+    }
     const float r0 = fmaf(fz, a1 - a0, a0), r1 = fmaf(fz, b1 - b0, b0);
     return fmaf(fo, r1 - r0, r0);
 }
@@ -223,12 +232,12 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs p) {
                 p0 = ldq<TV>(quads, ia);
                 p1 = ldq<TV>(quads, ia + FP);
             }
-            sa += tri(p0, p1, ff.x, fz.x, fo.x);
+            sa += tri<TV>(p0, p1, ff.x, fz.x, fo.x);
             if (ib != ia) {
                 p0 = ldq<TV>(quads, ib);
                 p1 = ldq<TV>(quads, ib + FP);
             }
-            sb += tri(p0, p1, ff.y, fz.y, fo.y);
+            sb += tri<TV>(p0, p1, ff.y, fz.y, fo.y);
             pidx = ib;
         }
         sum = sa + sb;
@@ -239,7 +248,7 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs p) {
             const float qz = fminf(fmaxf(fmaf(kf, vz, q0z), 0.f), mz);
             const float tf = __fadd_rz(qf, M), to = __fadd_rz(qo, M), tz = __fadd_rz(qz, M);
             const uint32_t i = __float_as_uint(tf) + __float_as_uint(to) * FP + __float_as_uint(tz) * PL + bias;
-            sum += tri(ldq<TV>(quads, i), ldq<TV>(quads, i + FP), qf - (tf - M), qz - (tz - M), qo - (to - M));
+            sum += tri<TV>(ldq<TV>(quads, i), ldq<TV>(quads, i + FP), qf - (tf - M), qz - (tz - M), qo - (to - M));
         }
     }
     const double dl = sqrt(vec[0] * p.dVX * vec[0] * p.dVX + vec[1] * p.dVY * vec[1] * p.dVY +

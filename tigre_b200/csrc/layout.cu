@@ -9,6 +9,8 @@
 // pad_projections builds the zero-bordered projection stack of the
 // backprojector (1 pixel before, 2 after, in u and v).
 
+#include <type_traits>
+
 #include "tigre_internal.h"
 
 namespace tigre {
@@ -77,7 +79,10 @@ __global__ void make_zfast_kernel(const Ts* __restrict__ src, T* __restrict__ ds
 // layout 1: y fastest; F = padded fast extent, O = padded other extent, Z = padded z extent),
 // element i = (p[i], p[i+1], p[i+F*O], p[i+1+F*O]) -- the fast-axis x z 2x2 corner block of
 // a trilinear sample, read as one vector load.  Corners past the last fast or z index are 0
-// (no sample has its base there).
+// (no sample has its base there).  FP32 quads hold the fast-axis differences instead of the
+// second corners, (p[i], p[i+1] - p[i], p[i+F*O], p[i+1+F*O] - p[i+F*O]), rounded to FP32 as
+// the sampler's own subtraction would be: each fast-axis lerp is then one FMA, with the same
+// result.
 template <typename T>
 struct Quad4 { T v[4]; };
 
@@ -94,6 +99,10 @@ __global__ void make_quads_kernel(const Ts* __restrict__ pad, Quad4<T>* __restri
         q.v[1] = f1 ? cv(pad[i + 1]) : from_f32<T>(0.f);
         q.v[2] = z1 ? cv(pad[i + plane]) : from_f32<T>(0.f);
         q.v[3] = (f1 && z1) ? cv(pad[i + plane + 1]) : from_f32<T>(0.f);
+        if constexpr (std::is_same<T, float>::value) {
+            q.v[1] = __fsub_rn(q.v[1], q.v[0]);
+            q.v[3] = __fsub_rn(q.v[3], q.v[2]);
+        }
         dst[i] = q;
     }
 }
