@@ -277,8 +277,10 @@ def measure_cgls():
     model = WS.pretrained_c5()
     if model is not None:
         out["warm_start"] = ("3-D U-Net (4 levels, 16 base channels, BF16, FP32 accumulation) trained by this "
-                             "library's kernels on 96 seeded 256^3 phantoms of this configuration (I0 = 5e4), "
-                             "weights in tigre_b200/data; its inference is timed with FDK")
+                             "library's kernels on 96 seeded 256^3 phantoms of this configuration (48 noisy at "
+                             "I0 = 5e4, 48 noiseless; image loss, then the relative residual after 4-5 unrolled "
+                             "CGLS iterations from its output), weights in tigre_b200/data; its inference is "
+                             "timed with FDK")
         with torch.no_grad():
             model(torch.zeros((C5_VOX,) * 3, device="cuda"))     # warm-up of the inference kernels
 
@@ -583,7 +585,7 @@ def main():
 # proportional to the view count (the Siddon grid reuses voxel columns across a tile of 64 views
 # in L2; the backprojector reads each view's patches once per voxel block), so the figure is
 # reported only for that exact launch.
-TRAFFIC_720_VIEWS = {"siddon": 6644203008 + 2288307968, "bp": 17286047744 + 527202816}
+TRAFFIC_720_VIEWS = {"siddon": 6589300736 + 2287803648, "bp": 22228711168 + 525339136}
 
 
 TRAFFIC_SOURCE = ("dram__bytes_read.sum + dram__bytes_write.sum of a single-pass ncu capture of the 720-view "

@@ -154,6 +154,18 @@ def test_warmstart_end_to_end_small():
     del torch
 
 
+def test_warmstart_unrolled_cgls_training_small():
+    """32^3: the data term through unrolled CGLS iterations (noiseless pairs) trains: the loss
+    falls, and every gradient reaches the network through the projector pair's autograd
+    Functions."""
+    from tigre_b200 import warmstart as WS
+    model = WS.unet(base=8, levels=3)
+    tr = WS.train(model, n_train=4, steps=40, n=32, crop=0, lr=2e-3, physics=1e4, unroll=3, clean_frac=1.0,
+                  img_weight=0.1)
+    assert np.isfinite(tr["loss_last"]) and tr["loss_last"] < tr["loss_first"], tr
+    assert all(p.grad is not None and bool(p.grad.abs().sum() > 0) for p in model.parameters())
+
+
 def test_unet_glue_kernels_match_torch():
     """pool2 / up_concat / conv_in / conv_out of the fused inference pass against the same
     operations in PyTorch (FP32 reference on the same BF16 values)."""
@@ -242,8 +254,8 @@ def test_unet_fused_inference_matches_autograd_forward():
 def test_pretrained_warm_start_saves_cgls_iterations():
     """The committed U-Net (trained on the warm-start configuration: 256^3, 512^2 detector at
     0.8 mm, 90 views, I0 = 5e4) on an unseen phantom of that configuration: CGLS started from its
-    output reaches the residual target in fewer iterations than from zero, with noisy data
-    (target: 100 zero-start iterations + 0.1 %) and noiseless data (target 5e-3)."""
+    output reaches the residual target in at most 60 % of the iterations from zero, with noisy
+    data (target: 100 zero-start iterations + 0.1 %) and noiseless data (target 5e-3)."""
     import torch
     from tigre_b200 import warmstart as WS
     model = WS.pretrained_c5()
@@ -253,5 +265,5 @@ def test_pretrained_warm_start_saves_cgls_iterations():
         row = ev["cases"][0]
         print("target %s: zero %d, FDK %d, warm %d iterations" % (
             target, row["plain_zero"]["iters"], row["plain_fdk"]["iters"], row["warm"]["iters"]))
-        assert row["warm"]["reached"] and row["warm"]["iters"] < row["plain_zero"]["iters"], row
+        assert row["warm"]["reached"] and row["warm"]["iters"] <= 0.6 * row["plain_zero"]["iters"], row
     del torch
