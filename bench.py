@@ -597,7 +597,7 @@ TRAFFIC_SOURCE = ("dram__bytes_read.sum + dram__bytes_write.sum of a single-pass
 # traffic is 0.6 % of its algorithmic bytes: it is bound by instruction issue and on-chip load
 # latency; the backprojector reads its taps from shared memory: bound by shared wavefronts and issue.
 PROFILED = {"siddon": {"warp_inst_per_view": 6.127e9 / 36, "source": "profiles/siddon_cells_512cube_36views.txt"},
-            "bp": {"warp_inst_per_view": 3.120e9 / 36, "wavefronts_per_view": 7.603e8 / 36,
+            "bp": {"warp_inst_per_view": 2.949e9 / 36, "wavefronts_per_view": 7.605e8 / 36,
                    "ideal_wavefronts_per_view": 512 ** 3 * 4 / 32,
                    "source": "profiles/bp_tma_matched_512cube_36views.txt"}}
 
