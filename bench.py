@@ -302,6 +302,7 @@ def measure_cgls():
         b = clean if variant == "noiseless" else torch.from_numpy(c5_noise(clean.cpu().numpy())).cuda()
         prob = Problem(b, geo, ang)
         cgls_device(prob, 3)                       # warm-up: plan, scratch, pools
+        fdk_device(prob)                           # warm-up: the filter's FFT plans
         if variant == "noiseless":
             target, crit = C5_TOL, "||b - Ax|| / ||b|| <= 5e-3 (1e-3 lies below the stall of CGLS over this pair)"
         else:
